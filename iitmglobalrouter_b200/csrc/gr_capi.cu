@@ -1,0 +1,646 @@
+// gr_capi.cu -- host side of the C ABI declared in include/iitmgr_b200.h.
+//
+// A context owns the grid state on one device and one stream:
+//   cap0, capr (int32 remaining capacity), fen (FP32 Fenwick nodes),
+//   a one-bit-per-cell mark bitmap and the list of cells marked in a batch.
+// Every batch runs as a fixed sequence of kernels on that stream with no
+// host synchronisation; batch sizes are known on the host from the design's
+// pin offsets, so launches (and captured graphs) need no device readback.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/iitmgr_b200.h"
+#include "gr_kernels.cuh"
+
+using namespace gr;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// batch descriptor arrays (host or device), SoA
+struct DescHost {
+    std::vector<int32_t> npin;
+    std::vector<int64_t> pin_base, pair_ofs, node_ofs, tab_ofs;
+};
+
+struct BatchInfo {  // one batch of a plan
+    int64_t first;  // index of its first net in the plan arrays
+    int32_t n;
+    int64_t n_pairs, n_nodes, n_tab, slot0;
+    int32_t max_pins;
+};
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    int32_t b0 = -1, b1 = -1;
+    void *mst = nullptr, *pat = nullptr;
+    cudaStream_t stream = nullptr;
+    int64_t launches = 0;
+};
+
+}  // namespace
+
+struct gr_ctx {
+    int device = 0, sm_count = 148;
+    GridC g{};
+    int64_t csize = 0;
+    cudaStream_t stream = nullptr;
+    // grid state
+    int32_t *d_cap0 = nullptr, *d_capr = nullptr;
+    float *d_fen = nullptr, *d_lut = nullptr;
+    uint32_t *d_mark = nullptr, *d_status = nullptr;
+    int32_t *d_owned = nullptr, *d_owned_count = nullptr;
+    std::vector<int32_t> h_cap0;
+    // design
+    int32_t n_nets = 0;
+    std::vector<int64_t> h_pin_ofs;
+    int32_t *d_pins = nullptr;
+    // per-call batch descriptor (device) + pinned staging
+    DevBuf desc, pcost, ppat, tab, dist;
+    void *h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    cudaEvent_t stage_done = nullptr;
+    // plan
+    std::vector<BatchInfo> plan;
+    DevBuf plan_desc;
+    int64_t plan_nets = 0, plan_slots = 0;
+    int64_t plan_max_pairs = 0, plan_max_tab = 0, plan_max_nets = 0;
+    GraphCache graph;
+    int64_t launches = 0;
+    int mst_smem_max = 0;
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+
+#define GR_CK(call)                                                                            \
+    do {                                                                                       \
+        cudaError_t _e = (call);                                                               \
+        if (_e != cudaSuccess) {                                                               \
+            fprintf(stderr, "iitmgr_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(_e), \
+                    __FILE__, __LINE__);                                                       \
+            return GR_ERR_CUDA;                                                                \
+        }                                                                                      \
+    } while (0)
+
+int grid_for(const gr_ctx *c, int64_t items, int per_sm = 8) {
+    int64_t b = (items + kThreads - 1) / kThreads;
+    int64_t cap = (int64_t)c->sm_count * per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int ensure(DevBuf &b, size_t bytes, cudaStream_t s) {
+    if (bytes <= b.bytes) return GR_OK;
+    if (b.p) {
+        GR_CK(cudaStreamSynchronize(s));
+        GR_CK(cudaFree(b.p));
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        return GR_ERR_NOMEM;
+    }
+    b.bytes = want;
+    return GR_OK;
+}
+
+cudaStream_t pick(gr_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
+
+int64_t tab_entries(const gr_ctx *c, int n) {
+    return n <= kTableMaxPins ? (int64_t)c->g.Z * n * n : 0;
+}
+
+// bytes of a SoA descriptor of n nets
+size_t desc_bytes(int64_t n) { return (size_t)n * (sizeof(int32_t) + 4 * sizeof(int64_t)) + 64; }
+
+// lays the SoA arrays of n nets out in a buffer (int64 arrays first)
+BatchView view_of(void *buf, int64_t total_n, int64_t first, int32_t n) {
+    char *p = (char *)buf;
+    BatchView v{};
+    int64_t *pin_base = (int64_t *)p;
+    int64_t *pair_ofs = pin_base + total_n;
+    int64_t *node_ofs = pair_ofs + total_n;
+    int64_t *tab_ofs = node_ofs + total_n;
+    int32_t *npin = (int32_t *)(tab_ofs + total_n);
+    v.n = n;
+    v.npin = npin + first;
+    v.pin_base = pin_base + first;
+    v.pair_ofs = pair_ofs + first;
+    v.node_ofs = node_ofs + first;
+    v.tab_ofs = tab_ofs + first;
+    return v;
+}
+
+// Builds the descriptor of one batch into `dst` (host SoA of total_n nets,
+// entries [first, first+n)). Returns GR_OK or GR_ERR_ARG / GR_ERR_STATE.
+int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t total_n, int64_t first,
+              BatchInfo &bi) {
+    BatchView v = view_of(dst, total_n, first, n);
+    int64_t *pin_base = const_cast<int64_t *>(v.pin_base);
+    int64_t *pair_ofs = const_cast<int64_t *>(v.pair_ofs);
+    int64_t *node_ofs = const_cast<int64_t *>(v.node_ofs);
+    int64_t *tab_ofs = const_cast<int64_t *>(v.tab_ofs);
+    int32_t *npin = const_cast<int32_t *>(v.npin);
+    int64_t P = 0, M = 0, T = 0;
+    int32_t mp = 0;
+    for (int32_t i = 0; i < n; i++) {
+        int32_t id = ids[i];
+        if (id < 0 || id >= c->n_nets) return GR_ERR_ARG;
+        int64_t o = c->h_pin_ofs[id];
+        int32_t k = (int32_t)(c->h_pin_ofs[id + 1] - o);
+        npin[i] = k;
+        pin_base[i] = o;
+        pair_ofs[i] = P;
+        node_ofs[i] = M;
+        tab_ofs[i] = T;
+        P += (int64_t)k * (k - 1) / 2;
+        M += k;
+        T += tab_entries(c, k);
+        if (k > mp) mp = k;
+    }
+    bi.first = first;
+    bi.n = n;
+    bi.n_pairs = P;
+    bi.n_nodes = M;
+    bi.n_tab = T;
+    bi.max_pins = mp;
+    return GR_OK;
+}
+
+BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
+    BatchView v = view_of(dev, total_n, bi.first, bi.n);
+    v.n_pairs = bi.n_pairs;
+    v.n_nodes = bi.n_nodes;
+    v.n_tab = bi.n_tab;
+    v.max_pins = bi.max_pins;
+    return v;
+}
+
+size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long long) + 5 * sizeof(int)); }
+
+// ------------------------------------------------------------------ stages
+
+int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s) {
+    if (v.n_tab > 0) {
+        k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab);
+        c->launches++;
+    }
+    if (v.n_pairs > 0) {
+        k_lpat_batch<<<grid_for(c, v.n_pairs, 16), kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost,
+                                                                    ppat);
+        c->launches++;
+    }
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s) {
+    if (v.n <= 0) return GR_OK;
+    size_t sm = mst_smem(v.max_pins);
+    int blocks = v.n < c->sm_count * 16 ? v.n : c->sm_count * 16;
+    k_mst<<<blocks, kThreads, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+    c->launches++;
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
+                  cudaStream_t s) {
+    if (v.n_nodes <= 0) return GR_OK;
+    GR_CK(cudaMemsetAsync(c->d_owned_count, 0, sizeof(int32_t), s));
+    Marker m{c->d_mark, c->d_owned, c->d_owned_count};
+    k_mark<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, m, c->d_status);
+    k_fen_update<<<c->sm_count * 4, kThreads, 0, s>>>(c->g, c->d_owned, c->d_owned_count, c->d_mark, c->d_capr,
+                                                       c->d_lut, c->d_fen);
+    k_finalize<<<c->sm_count * 4, kThreads, 0, s>>>(c->d_owned, c->d_owned_count, c->d_mark, c->d_capr);
+    c->launches += 3;
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int check_mst_smem(gr_ctx *c, int max_pins) {
+    if (max_pins > GR_MAX_PINS) return GR_ERR_NET_TOO_LARGE;
+    return GR_OK;
+}
+
+// scratch for one batch of the given sizes
+int ensure_scratch(gr_ctx *c, int64_t pairs, int64_t tab, int64_t nets, cudaStream_t s) {
+    int rc;
+    if ((rc = ensure(c->pcost, sizeof(float) * (pairs + 1), s))) return rc;
+    if ((rc = ensure(c->ppat, sizeof(int16_t) * (pairs + 1), s))) return rc;
+    if ((rc = ensure(c->tab, sizeof(float2) * (tab + 1), s))) return rc;
+    if ((rc = ensure(c->dist, sizeof(float) * (nets + 1), s))) return rc;
+    return GR_OK;
+}
+
+// copies the descriptor of a per-call batch to the device; returns its info
+int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchView &v, cudaStream_t s) {
+    if (!c->d_pins) return GR_ERR_STATE;
+    if (n < 0 || (n > 0 && !ids)) return GR_ERR_ARG;
+    size_t bytes = desc_bytes(n > 0 ? n : 1);
+    if (bytes > c->h_stage_bytes) {
+        if (c->h_stage) {
+            GR_CK(cudaEventSynchronize(c->stage_done));
+            GR_CK(cudaFreeHost(c->h_stage));
+        }
+        c->h_stage = nullptr;
+        if (cudaMallocHost(&c->h_stage, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            c->h_stage_bytes = 0;
+            return GR_ERR_NOMEM;
+        }
+        c->h_stage_bytes = bytes;
+    } else {
+        GR_CK(cudaEventSynchronize(c->stage_done));  // previous copy out of staging done
+    }
+    int rc = fill_desc(c, ids, n, c->h_stage, n, 0, bi);
+    if (rc) return rc;
+    if ((rc = check_mst_smem(c, bi.max_pins))) return rc;
+    if ((rc = ensure(c->desc, bytes, s))) return rc;
+    GR_CK(cudaMemcpyAsync(c->desc.p, c->h_stage, bytes, cudaMemcpyHostToDevice, s));
+    GR_CK(cudaEventRecord(c->stage_done, s));
+    v = make_view(c->desc.p, n, bi);
+    return GR_OK;
+}
+
+int route_one(gr_ctx *c, const BatchView &v, int64_t *mst, int32_t *mst_pat, float *dist, float *pcost,
+              int16_t *ppat, cudaStream_t s) {
+    int rc;
+    if ((rc = launch_lpat_batch(c, v, pcost, ppat, (float2 *)c->tab.p, s))) return rc;
+    if ((rc = launch_mst(c, v, pcost, mst, dist, s))) return rc;
+    return launch_commit(c, v, mst, ppat, mst_pat, s);
+}
+
+void free_buf(DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+void drop_graph(gr_ctx *c) {
+    if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
+    c->graph = GraphCache{};
+}
+
+}  // namespace
+
+// ====================================================================== API
+
+extern "C" {
+
+int gr_version(void) { return 1; }
+
+const char *gr_error_string(int code) {
+    switch (code) {
+        case GR_OK: return "ok";
+        case GR_ERR_ARG: return "invalid argument";
+        case GR_ERR_CUDA: return "CUDA runtime error";
+        case GR_ERR_NOMEM: return "out of memory";
+        case GR_ERR_STATE: return "call out of order";
+        case GR_ERR_NET_TOO_LARGE: return "net has more pins than supported";
+        case GR_ERR_DEVICE: return "a kernel reported invalid data";
+        case GR_ERR_IO: return "file could not be read or written";
+        case GR_ERR_PARSE: return "malformed input text";
+        case GR_ERR_NONINTEGER: return "capacity is not an integer";
+        default: return "unknown error";
+    }
+}
+
+int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_cap) {
+    if (!out || !h_cap || X < 1 || Y < 1 || Z < 3) return GR_ERR_ARG;
+    int64_t csize = (int64_t)X * Y * Z;
+    if (csize >= 0x7fffff00LL) return GR_ERR_ARG;  // cell ids are int32
+    *out = nullptr;
+    GR_CK(cudaSetDevice(device));
+    gr_ctx *c = new gr_ctx();
+    c->device = device;
+    c->g.X = X;
+    c->g.Y = Y;
+    c->g.Z = Z;
+    c->g.Z2 = (Z + 1) / 2;
+    c->g.npat = Z * c->g.Z2;
+    c->g.XY = X * Y;
+    c->csize = csize;
+    int rc = GR_OK;
+    auto fail = [&](int code) {
+        gr_destroy(c);
+        return code;
+    };
+    if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GR_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
+    size_t cell4 = sizeof(int32_t) * csize;
+    size_t words = (size_t)(csize / 32 + 2);
+    if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owned, cell4) ||
+        cudaMalloc(&c->d_owned_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
+        cudaGetLastError();
+        return fail(GR_ERR_NOMEM);
+    }
+    // cost LUT: (float)exp(-0.5 c) for integer remaining capacity c
+    std::vector<float> lut(kLutMax - kLutMin + 1);
+    for (int cc = kLutMin; cc <= kLutMax; cc++) lut[cc - kLutMin] = (float)std::exp(-0.5 * (double)cc);
+    c->h_cap0.assign(h_cap, h_cap + csize);
+    if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
+        cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
+        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
+        cudaMemset(c->d_owned_count, 0, 16))
+        return fail(GR_ERR_CUDA);
+    c->mst_smem_max = (int)mst_smem(GR_MAX_PINS);
+    if (cudaFuncSetAttribute(k_mst, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
+    if ((rc = gr_reset(c, nullptr))) return fail(rc);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);
+    *out = c;
+    return GR_OK;
+}
+
+int gr_destroy(gr_ctx *c) {
+    if (!c) return GR_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    cudaFree(c->d_cap0);
+    cudaFree(c->d_capr);
+    cudaFree(c->d_fen);
+    cudaFree(c->d_lut);
+    cudaFree(c->d_mark);
+    cudaFree(c->d_status);
+    cudaFree(c->d_owned);
+    cudaFree(c->d_owned_count);
+    cudaFree(c->d_pins);
+    free_buf(c->desc);
+    free_buf(c->pcost);
+    free_buf(c->ppat);
+    free_buf(c->tab);
+    free_buf(c->dist);
+    free_buf(c->plan_desc);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->stage_done) cudaEventDestroy(c->stage_done);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GR_OK;
+}
+
+int gr_reset(gr_ctx *c, void *stream) {
+    if (!c) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
+    GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
+    k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
+    c->launches++;
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins) {
+    if (!c || n_nets < 0 || !h_pin_ofs || (n_nets > 0 && !h_pins) || h_pin_ofs[0] != 0) return GR_ERR_ARG;
+    for (int32_t i = 0; i < n_nets; i++) {
+        int64_t k = h_pin_ofs[i + 1] - h_pin_ofs[i];
+        if (k < 2) return GR_ERR_ARG;
+        if (k > GR_MAX_PINS) return GR_ERR_NET_TOO_LARGE;
+    }
+    int64_t total = h_pin_ofs[n_nets];
+    for (int64_t t = 0; t < total; t++)
+        if (h_pins[t] < 0 || h_pins[t] >= c->csize) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);
+    if (c->d_pins) cudaFree(c->d_pins);
+    c->d_pins = nullptr;
+    if (cudaMalloc(&c->d_pins, sizeof(int32_t) * (total + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return GR_ERR_NOMEM;
+    }
+    GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    c->h_pin_ofs.assign(h_pin_ofs, h_pin_ofs + n_nets + 1);
+    c->n_nets = n_nets;
+    c->plan.clear();
+    GR_CK(cudaStreamSynchronize(c->stream));
+    return GR_OK;
+}
+
+int gr_lpattern(gr_ctx *c, const int32_t *d_pairs, int64_t n_pairs, float *d_cost, int16_t *d_pat, void *stream) {
+    if (!c || n_pairs < 0 || (n_pairs > 0 && (!d_pairs || !d_cost || !d_pat))) return GR_ERR_ARG;
+    if (n_pairs == 0) return GR_OK;
+    cudaStream_t s = pick(c, stream);
+    k_lpat_pairs<<<grid_for(c, n_pairs, 16), kThreads, 0, s>>>(c->g, (int)c->csize, d_pairs, n_pairs, c->d_fen,
+                                                              d_cost, d_pat, c->d_status);
+    c->launches++;
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int gr_brvsk_build(gr_ctx *c, const int32_t *h_net_ids, int32_t n_nets, const float *d_pair_cost,
+                   int64_t *d_mst_edges, float *d_net_dist, void *stream) {
+    if (!c || !d_pair_cost || !d_mst_edges) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    BatchInfo bi{};
+    BatchView v{};
+    int rc = upload_batch(c, h_net_ids, n_nets, bi, v, s);
+    if (rc) return rc;
+    return launch_mst(c, v, d_pair_cost, d_mst_edges, d_net_dist, s);
+}
+
+int gr_mst_bit_commit(gr_ctx *c, const int32_t *h_net_ids, int32_t n_nets, const int64_t *d_mst_edges,
+                      const int16_t *d_pair_pat, int32_t *d_mst_pat, void *stream) {
+    if (!c || !d_mst_edges || !d_pair_pat) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    BatchInfo bi{};
+    BatchView v{};
+    int rc = upload_batch(c, h_net_ids, n_nets, bi, v, s);
+    if (rc) return rc;
+    return launch_commit(c, v, d_mst_edges, d_pair_pat, d_mst_pat, s);
+}
+
+int gr_route_batch(gr_ctx *c, const int32_t *h_net_ids, int32_t n_nets, int64_t *d_mst_edges, int32_t *d_mst_pat,
+                   float *d_net_dist, float *d_pair_cost, int16_t *d_pair_pat, void *stream) {
+    if (!c || !d_mst_edges) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    BatchInfo bi{};
+    BatchView v{};
+    int rc = upload_batch(c, h_net_ids, n_nets, bi, v, s);
+    if (rc) return rc;
+    if ((rc = ensure_scratch(c, bi.n_pairs, bi.n_tab, n_nets, s))) return rc;
+    float *pc = d_pair_cost ? d_pair_cost : (float *)c->pcost.p;
+    int16_t *pp = d_pair_pat ? d_pair_pat : (int16_t *)c->ppat.p;
+    return route_one(c, v, d_mst_edges, d_mst_pat, d_net_dist, pc, pp, s);
+}
+
+int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const int32_t *h_net_ids) {
+    if (!c || n_batches < 0 || !h_batch_ofs || h_batch_ofs[0] != 0) return GR_ERR_ARG;
+    if (!c->d_pins) return GR_ERR_STATE;
+    int64_t total = h_batch_ofs[n_batches];
+    if (total < 0 || (total > 0 && !h_net_ids)) return GR_ERR_ARG;
+    for (int32_t b = 0; b < n_batches; b++)
+        if (h_batch_ofs[b + 1] < h_batch_ofs[b]) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    drop_graph(c);
+    size_t bytes = desc_bytes(total > 0 ? total : 1);
+    std::vector<char> host(bytes);
+    std::vector<BatchInfo> plan(n_batches);
+    int64_t slot = 0, mp = 0, mt = 0, mn = 0;
+    for (int32_t b = 0; b < n_batches; b++) {
+        int rc = fill_desc(c, h_net_ids + h_batch_ofs[b], (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]),
+                           host.data(), total, h_batch_ofs[b], plan[b]);
+        if (rc) return rc;
+        if ((rc = check_mst_smem(c, plan[b].max_pins))) return rc;
+        plan[b].slot0 = slot;
+        slot += plan[b].n_nodes;
+        if (plan[b].n_pairs > mp) mp = plan[b].n_pairs;
+        if (plan[b].n_tab > mt) mt = plan[b].n_tab;
+        if (plan[b].n > mn) mn = plan[b].n;
+    }
+    int rc;
+    if ((rc = ensure(c->plan_desc, bytes, c->stream))) return rc;
+    GR_CK(cudaMemcpyAsync(c->plan_desc.p, host.data(), bytes, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = ensure_scratch(c, mp, mt, mn, c->stream))) return rc;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    c->plan = std::move(plan);
+    c->plan_nets = total;
+    c->plan_slots = slot;
+    c->plan_max_pairs = mp;
+    c->plan_max_tab = mt;
+    c->plan_max_nets = mn;
+    return GR_OK;
+}
+
+int64_t gr_plan_slots(gr_ctx *c) { return c ? c->plan_slots : -1; }
+
+int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
+                  void *stream) {
+    if (!c || !d_mst_edges || b0 < 0 || b1 < b0 || b1 > (int32_t)c->plan.size()) return GR_ERR_ARG;
+    if (c->plan.empty() && b1 > 0) return GR_ERR_STATE;
+    cudaStream_t s = pick(c, stream);
+    auto issue = [&]() -> int {
+        for (int32_t b = b0; b < b1; b++) {
+            const BatchInfo &bi = c->plan[b];
+            BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
+            int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr,
+                               (float *)c->dist.p, (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
+            if (rc) return rc;
+        }
+        return GR_OK;
+    };
+    if (!(flags & GR_PLAN_GRAPH)) return issue();
+    GraphCache &gc = c->graph;
+    if (!(gc.exec && gc.b0 == b0 && gc.b1 == b1 && gc.mst == d_mst_edges && gc.pat == d_mst_pat &&
+          gc.stream == s)) {
+        drop_graph(c);
+        int64_t before = c->launches;
+        cudaGraph_t graph = nullptr;
+        GR_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int rc = issue();
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return GR_ERR_CUDA;
+        cudaError_t ie = cudaGraphInstantiate(&gc.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            gc.exec = nullptr;
+            return GR_ERR_CUDA;
+        }
+        gc.b0 = b0;
+        gc.b1 = b1;
+        gc.mst = d_mst_edges;
+        gc.pat = d_mst_pat;
+        gc.stream = s;
+        gc.launches = c->launches - before;
+        c->launches = before;
+    }
+    GR_CK(cudaGraphLaunch(gc.exec, s));
+    c->launches += gc.launches;
+    return GR_OK;
+}
+
+int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins,
+                         int32_t n_batches, const int64_t *h_batch_ofs, const int32_t *h_net_ids,
+                         int64_t *h_mst_edges, int32_t *h_mst_pat, int flags) {
+    if (!c || !h_mst_edges) return GR_ERR_ARG;
+    int rc;
+    if ((rc = gr_set_nets(c, n_nets, h_pin_ofs, h_pins))) return rc;
+    if ((rc = gr_plan_set(c, n_batches, h_batch_ofs, h_net_ids))) return rc;
+    if ((rc = gr_reset(c, nullptr))) return rc;
+    int64_t slots = c->plan_slots;
+    DevBuf mst, pat;
+    if ((rc = ensure(mst, sizeof(int64_t) * (slots + 1), c->stream)) ||
+        (rc = ensure(pat, sizeof(int32_t) * (slots + 1), c->stream))) {
+        free_buf(mst);
+        free_buf(pat);
+        return rc;
+    }
+    rc = gr_route_plan(c, 0, n_batches, (int64_t *)mst.p, (int32_t *)pat.p, flags & ~GR_PLAN_GRAPH, nullptr);
+    if (!rc) {
+        cudaMemcpyAsync(h_mst_edges, mst.p, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream);
+        if (h_mst_pat) cudaMemcpyAsync(h_mst_pat, pat.p, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream);
+        rc = gr_sync(c);
+    }
+    cudaStreamSynchronize(c->stream);
+    free_buf(mst);
+    free_buf(pat);
+    return rc;
+}
+
+int gr_sync(gr_ctx *c) {
+    if (!c) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    return gr_status(c) ? GR_ERR_DEVICE : GR_OK;
+}
+
+uint32_t gr_status(gr_ctx *c) {
+    if (!c) return 0;
+    uint32_t st = 0;
+    if (cudaMemcpyAsync(&st, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+        return 0xffffffffu;
+    cudaStreamSynchronize(c->stream);
+    return st;
+}
+
+int gr_clear_status(gr_ctx *c) {
+    if (!c) return GR_ERR_ARG;
+    GR_CK(cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), c->stream));
+    return GR_OK;
+}
+
+int gr_get_capr(gr_ctx *c, int32_t *h_out) {
+    if (!c || !h_out) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    GR_CK(cudaMemcpy(h_out, c->d_capr, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToHost));
+    return GR_OK;
+}
+
+int gr_get_demand(gr_ctx *c, int32_t *h_out) {
+    int rc = gr_get_capr(c, h_out);
+    if (rc) return rc;
+    for (int64_t i = 0; i < c->csize; i++) h_out[i] = c->h_cap0[i] - h_out[i];
+    return GR_OK;
+}
+
+int gr_get_fenwick(gr_ctx *c, float *h_out) {
+    if (!c || !h_out) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    GR_CK(cudaMemcpy(h_out, c->d_fen, sizeof(float) * c->csize, cudaMemcpyDeviceToHost));
+    return GR_OK;
+}
+
+void *gr_stream(gr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int64_t gr_launch_count(gr_ctx *c) { return c ? c->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,228 @@
+// gr_device.cuh -- device-side building blocks of the routing hot path.
+//
+// Grid encoding follows the reference (util.hpp:37-68, WIRE_ENC): every
+// routing track (row on even layers, column on odd layers) is contiguous, so
+// the Fenwick node i (1-based) of a track lives at cell (track base + i - 1)
+// exactly as in bit_util.hpp:19-55.
+//
+// All floating-point sums are written so that the sequence of IEEE FP32
+// additions equals the reference's sequential code (and the CPU oracle):
+// prefix queries add nodes from index pos+1 downwards, pattern costs add
+// terms in path order. Nothing here may be reassociated.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gr {
+
+constexpr int kLutMin = -256;  // cost LUT covers remaining capacity [-256, 1024]
+constexpr int kLutMax = 1024;
+constexpr int kTableMaxPins = 1024;  // nets above this use direct Fenwick gathers
+constexpr int kMstMaxRounds = 40;
+
+struct GridC {
+    int X, Y, Z, Z2, npat;
+    int XY;
+};
+
+__device__ __forceinline__ void dec(const GridC &g, int32_t e, int &z, int &x, int &y) {
+    z = e / g.XY;
+    int r = e - z * g.XY;
+    if (z & 1) {
+        x = r / g.Y;
+        y = r - x * g.Y;
+    } else {
+        y = r / g.X;
+        x = r - y * g.X;
+    }
+}
+
+__device__ __forceinline__ int32_t enc(const GridC &g, int z, int x, int y) {
+    return (z & 1) ? z * g.XY + x * g.Y + y : z * g.XY + y * g.X + x;
+}
+
+// base cell of the track through (z, x, y)
+__device__ __forceinline__ int32_t track_base(const GridC &g, int z, int x, int y) {
+    return (z & 1) ? z * g.XY + x * g.Y : z * g.XY + y * g.X;
+}
+
+// Inclusive prefix query of one track (bit_util.hpp:19-35): nodes from
+// index pos+1 down to 1, accumulated in that order starting from 0.
+__device__ __forceinline__ float fen_query(const float *__restrict__ fen, int32_t base, int pos) {
+    float res = 0.0f;
+    for (int i = pos + 1; i > 0; i &= i - 1) res += __ldg(fen + base + i - 1);
+    return res;
+}
+
+// Order-preserving 64-bit key of (cost, pair id): the Boruvka minimum is
+// the smallest cost, ties broken by the lowest pair id.
+__device__ __forceinline__ unsigned long long cost_key(float w, uint32_t e) {
+    if (w == 0.0f) w = 0.0f;  // -0 == +0 in the reference's comparisons
+    uint32_t u = __float_as_uint(w);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)u << 32) | (unsigned long long)e;
+}
+
+// decode a local pair id e = j(j-1)/2 + k (k < j), gmst_util.hpp:192-194
+__device__ __forceinline__ void pair_decode(long long e, int &j, int &k) {
+    long long jj = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);
+    while (jj * (jj - 1) / 2 > e) jj--;
+    while ((jj + 1) * jj / 2 <= e) jj++;
+    j = (int)jj;
+    k = (int)(e - jj * (jj - 1) / 2);
+}
+
+// largest i in [0, n) with ofs[i] <= t (ofs ascending, ofs[0] == 0)
+__device__ __forceinline__ int ofs_search(const int64_t *__restrict__ ofs, int n, int64_t t) {
+    int lo = 0, hi = n;  // invariant: ofs[lo] <= t, answer in [lo, hi)
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(ofs + mid) <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// L-pattern evaluation (bit_util.hpp:134-191), generic over how prefix
+// queries are answered. Ev provides:
+//   z1, z2, bth                       source layer, target layer, both x and y differ
+//   State start()                     position at the source pin
+//   void via(za, zb, State, float&)   point costs of layers [min, max) at State
+//   void wire(z, State&, float&)      wire on layer z to the target's coordinate
+//   bool at_dst(State)
+// The pattern loop shares the (via1, first wire) prefix across the ceil(Z/2)
+// second-via choices; the prefix value is the same FP32 partial sum the
+// reference computes per thread, so costs are unchanged.
+template <class Ev>
+__device__ __forceinline__ void lpat_argmin(const Ev &ev, const GridC &g, float &out_c, int &out_p) {
+    float best = __int_as_float(0x7f800000);
+    int bp = -1, first = -1;
+    for (int via1 = 1; via1 < g.Z; via1++) {
+        typename Ev::State st = ev.start();
+        float c0 = 0.0f;
+        int zs = ev.z1;
+        if (zs != via1) {
+            ev.via(zs, via1, st, c0);
+            zs = via1;
+        }
+        ev.wire(zs, st, c0);
+        for (int v = 0; v < g.Z2; v++) {
+            const int cpat = via1 * g.Z2 + v;
+            float c = c0;
+            typename Ev::State s2 = st;
+            int z = zs;
+            const int via2 = (z & 1) ? 2 * v : 2 * v + 1;
+            if (ev.bth && via2 != 0) {
+                if (via2 >= g.Z) continue;  // odd Z: layer Z does not exist
+                if (z != via2) {
+                    ev.via(z, via2, s2, c);
+                    z = via2;
+                    ev.wire(z, s2, c);
+                }
+            }
+            if (z != ev.z2) ev.via(z, ev.z2, s2, c);
+            if (!ev.at_dst(s2)) continue;
+            if (first < 0) first = cpat;
+            if (c < best) {
+                best = c;
+                bp = cpat;
+            }
+        }
+    }
+    if (bp < 0) {
+        bp = first;
+        best = __int_as_float(0x7f800000);
+    }
+    out_c = best;
+    out_p = bp;
+}
+
+// Prefix queries answered straight from the Fenwick array (any pair).
+struct DirectEv {
+    struct State {
+        int x, y;
+    };
+    const float *fen;
+    GridC g;
+    int z1, x1, y1, z2, x2, y2;
+    bool bth;
+    __device__ State start() const { return State{x1, y1}; }
+    __device__ float point(int z, int x, int y) const {
+        int32_t b = track_base(g, z, x, y);
+        int p = (z & 1) ? y : x;
+        float hi = fen_query(fen, b, p);
+        float lo = fen_query(fen, b, p - 1);
+        return hi - lo;
+    }
+    __device__ void via(int za, int zb, State s, float &c) const {
+        int zmin = za < zb ? za : zb, zmax = za < zb ? zb : za;
+        for (int i = zmin; i < zmax; i++) c += point(i, s.x, s.y);
+    }
+    __device__ void wire(int z, State &s, float &c) const {
+        int32_t b = track_base(g, z, s.x, s.y);
+        if (z & 1) {
+            if (s.y < y2) {
+                float hi = fen_query(fen, b, y2), lo = fen_query(fen, b, s.y - 1);
+                c += hi - lo;
+            } else if (s.y > y2) {
+                float hi = fen_query(fen, b, s.y), lo = fen_query(fen, b, y2 - 1);
+                c += hi - lo;
+            }
+            s.y = y2;
+        } else {
+            if (s.x < x2) {
+                float hi = fen_query(fen, b, x2), lo = fen_query(fen, b, s.x - 1);
+                c += hi - lo;
+            } else if (s.x > x2) {
+                float hi = fen_query(fen, b, s.x), lo = fen_query(fen, b, x2 - 1);
+                c += hi - lo;
+            }
+            s.x = x2;
+        }
+    }
+    __device__ bool at_dst(State s) const { return s.x == x2 && s.y == y2; }
+};
+
+// Prefix queries read from a per-net query table. For a net of n pins the
+// table holds, for every layer z and pin indices (a, b), the pair
+//   even z: (Q(z, row y_b, x_a), Q(z, row y_b, x_a - 1))
+//   odd  z: (Q(z, col x_a, y_b), Q(z, col x_a, y_b - 1))
+// at tab[(z*n + a)*n + b]. A pattern of pair (j -> k) only visits the four
+// points {x_j, x_k} x {y_j, y_k}, so every query it makes is in the table.
+struct TableEv {
+    struct State {
+        int a, b;  // pin index giving x, pin index giving y
+    };
+    const float2 *tab;
+    int n, j, k;
+    int z1, z2, xj, yj, xk, yk;
+    bool bth;
+    __device__ State start() const { return State{j, j}; }
+    __device__ float2 t(int z, int a, int b) const { return tab[((int64_t)z * n + a) * n + b]; }
+    __device__ int xof(int a) const { return a == j ? xj : xk; }
+    __device__ int yof(int b) const { return b == j ? yj : yk; }
+    __device__ void via(int za, int zb, State s, float &c) const {
+        int zmin = za < zb ? za : zb, zmax = za < zb ? zb : za;
+        for (int i = zmin; i < zmax; i++) {
+            float2 q = t(i, s.a, s.b);
+            c += q.x - q.y;
+        }
+    }
+    __device__ void wire(int z, State &s, float &c) const {
+        if (z & 1) {
+            int yb = yof(s.b);
+            if (yb < yk) c += t(z, s.a, k).x - t(z, s.a, s.b).y;
+            else if (yb > yk) c += t(z, s.a, s.b).x - t(z, s.a, k).y;
+            s.b = k;
+        } else {
+            int xa = xof(s.a);
+            if (xa < xk) c += t(z, k, s.b).x - t(z, s.a, s.b).y;
+            else if (xa > xk) c += t(z, s.a, s.b).x - t(z, k, s.b).y;
+            s.a = k;
+        }
+    }
+    __device__ bool at_dst(State s) const { return xof(s.a) == xk && yof(s.b) == yk; }
+};
+
+}  // namespace gr
