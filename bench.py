@@ -1,0 +1,352 @@
+"""Benchmark of the routing hot path (L-pattern -> Boruvka RMST -> Fenwick
+commit) on the 1.2M-net synthetic design, in nets/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+A step routes every batch of the design's -batch_part -num_xdim_parts 4 plan
+from the initial cost state (Fenwick rebuild included). Inputs are resident
+in HBM for `value`; `e2e` times the host-buffer C ABI call
+(gr_route_design_host) with the nets and plan copied in and the MST slots
+and patterns copied out every step. Multi-GPU runs are independent replicas
+(the path has no data-parallel split: batches are sequential through the
+shared cost state), so `value` is the whole-job throughput of N replicas.
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "nets/s (Lpat+MST+commit) on 1 B200; overflow & WL, learned vs plain cost"
+UNIT = "nets/s"
+WORKLOAD = "synthetic 1000x1000x10 GCELLs, cap U{8..16}, 1.2M nets (1% tail to 400 pins), -batch_part -num_xdim_parts 4"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def net_bytes(d, ofs, pins, total_demand):
+    """Sum over nets of B_net = 4*Z*w*h + 4*n + 12*(n-1) + 16*G_net."""
+    dims = d.dims
+    X, Y, Z = dims["X"], dims["Y"], dims["Z"]
+    XY = X * Y
+    z = pins // XY
+    r = pins % XY
+    x = np.where(z & 1, r // Y, r % X)
+    y = np.where(z & 1, r % Y, r // X)
+    seg = ofs[:-1]
+    w = np.maximum.reduceat(x, seg) - np.minimum.reduceat(x, seg) + 1
+    h = np.maximum.reduceat(y, seg) - np.minimum.reduceat(y, seg) + 1
+    n = np.diff(ofs)
+    return int(4 * Z * (w.astype(np.int64) * h).sum() + 4 * n.sum() + 12 * (n - 1).sum() + 16 * int(total_demand))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [ln.split(",") for ln in Path(self.f.name).read_text().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit())}
+
+
+def make_workload(config, seed):
+    import iitmglobalrouter_b200 as gr
+
+    d = gr.Design.generate(config, seed=seed)
+    bofs, ids = d.batch(4)
+    ofs, pins = d.nets()
+    return d, ofs, pins, bofs, ids
+
+
+def cpu_sample(ofs, pins, bofs, ids, target_pairs):
+    """Strided batches of the plan whose pairs add up to about target_pairs."""
+    import iitmglobalrouter_b200 as gr
+
+    nb = len(bofs) - 1
+    pairs = np.array([gr.pair_count(ofs, ids[bofs[b]:bofs[b + 1]]) for b in range(nb)])
+    stride = max(1, int(np.ceil(pairs.sum() / max(target_pairs, 1))))
+    sel = list(range(0, nb, stride))
+    sofs = [0]
+    sids = []
+    for b in sel:
+        sids.append(ids[bofs[b]:bofs[b + 1]])
+        sofs.append(sofs[-1] + len(sids[-1]))
+    return np.array(sofs, np.int64), np.concatenate(sids).astype(np.int32), stride, len(sel)
+
+
+def time_oracle(d, ofs, pins, sofs, sids, nthreads):
+    import oracle
+
+    dims = d.dims
+    g = oracle.Grid(dims["X"], dims["Y"], dims["Z"], d.caps())
+    t0 = time.perf_counter()
+    rc, _, _ = g.route_batches(ofs, pins, sofs, sids, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    assert rc == 0
+    return len(sids) / dt, dt
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's algorithm on the host cores (the
+    CPU oracle -- the reference's own GPU binary cannot be built here and its
+    sq_router CPU path does not compile)."""
+    if rank != 0:
+        return
+    d, ofs, pins, bofs, ids = make_workload(args.config, args.seed)
+    nthreads = os.cpu_count() or 1
+    sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
+    for _ in range(args.warmup):
+        time_oracle(d, ofs, pins, sofs, sids, nthreads)
+    times = []
+    for _ in range(args.steps):
+        times.append(time_oracle(d, ofs, pins, sofs, sids, nthreads)[1])
+    t = sum(times) / len(times)
+    v = len(sids) / t
+    sample = f"every {stride}th batch of the plan ({nsel} batches, {len(sids)} nets) routed in order"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "seed": args.seed, "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-pairs", type=int, default=2_000_000, help="pairs in the CPU oracle sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    import iitmglobalrouter_b200 as gr
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    d, ofs, pins, bofs, ids = make_workload(args.config, args.seed)
+    dims = d.dims
+    n_nets = dims["n_nets"]
+    cap = d.caps()
+    R = gr.Router(dims["X"], dims["Y"], dims["Z"], cap, device=local)
+    R.set_nets(ofs, pins)
+    R.plan_set(bofs, ids)
+    M = R.plan_slots
+    mst = torch.empty(M, dtype=torch.int64, device=dev)
+    pat = torch.empty(M, dtype=torch.int32, device=dev)
+    stream = torch.cuda.ExternalStream(R.stream, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step():
+        R.reset()
+        R.route_plan(mst, pat, graph=True)
+
+    for _ in range(args.warmup):
+        step()
+    R.sync()
+    if R.status():
+        raise SystemExit(f"device status {R.status():#x}")
+
+    # timed region: K steps, L2 flushed before each, CUDA events on the
+    # router's stream around each step
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    times = []
+    l0 = R.launch_count
+    with Clocks(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+    launches = R.launch_count - l0
+    clocks = clk.summary()
+    total_ms = float(sum(times))
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    value = world * n_nets * args.steps / (total_ms / 1e3)
+
+    # quality of the routed design (plain cost)
+    demand = R.demand()
+    q = d.evaluate(demand)
+    mst_h = mst.cpu().numpy()
+    pat_h = pat.cpu().numpy()
+    wl, vias = d.write_routes(os.devnull, mst_h, pat_h, merge=True, rseg=True, ppatch=True, threads=8)
+
+    # per-kernel breakdown: one profiled step (events around each launch)
+    R.reset()
+    R.sync()
+    R.profile(True)
+    R.profile_read(reset=True)
+    R.route_plan(mst, pat, graph=False)
+    kern = R.profile_read(reset=True)
+    R.profile(False)
+    kern_total = sum(v[0] for v in kern.values())
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / kern_total, 4)}
+               for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}
+    dominant = next(iter(kernels))
+
+    # roofline of the step (all kernels): algorithmic bytes per step / step time
+    bnet = net_bytes(d, ofs, pins, int(demand.sum()))
+    peak, peak_kind = peaks()
+    achieved = bnet / (ms_step / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "dram_traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        traffic = tj.get("bytes_per_step")
+
+    # end to end through the host-buffer C ABI call (pinned host memory)
+    def pinned(a):
+        t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        return t
+
+    h_ofs, h_pins, h_bofs, h_ids = pinned(ofs), pinned(pins), pinned(bofs), pinned(ids)
+    h_mst = torch.empty(M, dtype=torch.int64).pin_memory()
+    h_pat = torch.empty(M, dtype=torch.int32).pin_memory()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        barrier()
+        t0 = time.perf_counter()
+        R.route_design_host(h_ofs.numpy(), h_pins.numpy(), h_bofs.numpy(), h_ids.numpy(), h_mst.numpy(),
+                            h_pat.numpy())
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e_times.append(t1 - t0)
+    e2e_t = sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_t], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    assert np.array_equal(h_mst.numpy(), mst_h), "end-to-end result differs from the resident run"
+    h2d = pins.nbytes + (ids.size * 36 + 64)  # design pins + plan descriptor (pin offsets stay on the host)
+    d2h = M * 8 + M * 4
+
+    cpu = None
+    if rank == 0:
+        sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
+        nthreads = os.cpu_count() or 1
+        v_cpu, dt = time_oracle(d, ofs, pins, sofs, sids, nthreads)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"every {stride}th batch of the plan ({nsel} batches, {len(sids)} nets, {dt:.1f} s)"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nets": n_nets, "pins": dims["n_pins"], "pairs": gr.pair_count(ofs, ids),
+                   "batches": len(bofs) - 1, "seed": args.seed, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MB write) before every timed step", "graph": True},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": "route step (all kernels)",
+                     "algorithmic_bytes_per_step": bnet, "dominant_kernel": dominant},
+        "kernels": kernels,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * n_nets / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "quality": {"overflow": q["overflow"], "overflow_cells": q["overflow_cells"], "demand": q["demand"],
+                    "wirelength": wl, "vias": vias},
+    }
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -24,6 +24,7 @@ GR_ST_BAD_EDGE, GR_ST_BAD_PATTERN, GR_ST_MST_ROUNDS, GR_ST_BAD_PIN = 0x1, 0x2, 0
 GR_PLAN_GRAPH = 0x1
 GR_WRT_MERGE, GR_WRT_RSEG, GR_WRT_PPATCH = 0x1, 0x2, 0x4
 GR_MAX_PINS = 4096
+GR_PROF_KINDS = 8
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
 _P, _I, _I64, _U64, _D = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double
@@ -51,6 +52,9 @@ SIGNATURES = {
     "gr_get_fenwick": (_I, [_P, _P]),
     "gr_stream": (_P, [_P]),
     "gr_launch_count": (_I64, [_P]),
+    "gr_profile_enable": (_I, [_P, _I]),
+    "gr_profile_read": (_I, [_P, _P, _P, _I]),
+    "gr_kernel_name": (C.c_char_p, [_I]),
     "gr_design_generate": (_I, [_PP, _I, _U64, _I64]),
     "gr_design_generate_custom": (_I, [_PP, _I, _I, _I, _I, _I, _D, _I, _I, _I64, _D, _I, _D, _D, _I, _U64]),
     "gr_design_read": (_I, [_PP, C.c_char_p, C.c_char_p, _I]),

@@ -56,7 +56,7 @@ struct gr_ctx {
     int32_t *d_cap0 = nullptr, *d_capr = nullptr;
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
-    int32_t *d_owned = nullptr, *d_owned_count = nullptr;
+    int32_t *d_owner = nullptr;
     std::vector<int32_t> h_cap0;
     // design
     int32_t n_nets = 0;
@@ -75,6 +75,14 @@ struct gr_ctx {
     GraphCache graph;
     int64_t launches = 0;
     int mst_smem_max = 0;
+    // optional per-kernel timing (CUDA events around every launch)
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_kind;
+    size_t ev_used = 0;
+    double prof_ms[GR_PROF_KINDS] = {};
+    int64_t prof_n[GR_PROF_KINDS] = {};
+    size_t pins_cap = 0;
 };
 
 namespace {
@@ -97,6 +105,31 @@ int grid_for(const gr_ctx *c, int64_t items, int per_sm = 8) {
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
+}
+
+// Records an event before a launch when profiling (never inside a capture).
+int prof_begin(gr_ctx *c, cudaStream_t s) {
+    if (!c->profiling) return -1;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return -1;
+    if (c->ev_used + 2 > c->ev.size()) {
+        for (int i = 0; i < 256; i++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return -1;
+            c->ev.push_back(e);
+        }
+        c->ev_kind.resize(c->ev.size() / 2 + 1);
+    }
+    int i = (int)c->ev_used;
+    c->ev_used += 2;
+    cudaEventRecord(c->ev[i], s);
+    return i;
+}
+void prof_end(gr_ctx *c, cudaStream_t s, int i, int kind) {
+    c->launches++;
+    if (i < 0) return;
+    cudaEventRecord(c->ev[i + 1], s);
+    c->ev_kind[i / 2] = kind;
 }
 
 int ensure(DevBuf &b, size_t bytes, cudaStream_t s) {
@@ -194,13 +227,25 @@ size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long 
 
 int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s) {
     if (v.n_tab > 0) {
+        int pi = prof_begin(c, s);
         k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab);
-        c->launches++;
+        prof_end(c, s, pi, GR_K_QTABLE);
     }
     if (v.n_pairs > 0) {
-        k_lpat_batch<<<grid_for(c, v.n_pairs, 16), kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost,
-                                                                    ppat);
-        c->launches++;
+        int pi = prof_begin(c, s);
+        const int grid = grid_for(c, v.n_pairs, 16);
+#define GR_LPAT_Z(ZV)                                                                                 \
+    case ZV:                                                                                          \
+        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost, ppat);       \
+        break;
+        switch (c->g.Z) {
+            GR_LPAT_Z(3) GR_LPAT_Z(4) GR_LPAT_Z(5) GR_LPAT_Z(6) GR_LPAT_Z(7) GR_LPAT_Z(8) GR_LPAT_Z(9)
+            GR_LPAT_Z(10) GR_LPAT_Z(11) GR_LPAT_Z(12) GR_LPAT_Z(13) GR_LPAT_Z(14) GR_LPAT_Z(15) GR_LPAT_Z(16)
+            default:
+                k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost, ppat);
+        }
+#undef GR_LPAT_Z
+        prof_end(c, s, pi, GR_K_LPAT);
     }
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -208,10 +253,16 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
 
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s) {
     if (v.n <= 0) return GR_OK;
-    size_t sm = mst_smem(v.max_pins);
-    int blocks = v.n < c->sm_count * 16 ? v.n : c->sm_count * 16;
-    k_mst<<<blocks, kThreads, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
-    c->launches++;
+    int pi = prof_begin(c, s);
+    k_mst_small<<<grid_for(c, v.n, 8), kThreads, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+    prof_end(c, s, pi, GR_K_MST);
+    if (v.max_pins > kMstWarpPins) {
+        size_t sm = mst_smem(v.max_pins);
+        int blocks = v.n < c->sm_count * 8 ? v.n : c->sm_count * 8;
+        pi = prof_begin(c, s);
+        k_mst_large<<<blocks, kThreads, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+        prof_end(c, s, pi, GR_K_MST);
+    }
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -219,13 +270,17 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
                   cudaStream_t s) {
     if (v.n_nodes <= 0) return GR_OK;
-    GR_CK(cudaMemsetAsync(c->d_owned_count, 0, sizeof(int32_t), s));
-    Marker m{c->d_mark, c->d_owned, c->d_owned_count};
-    k_mark<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, m, c->d_status);
-    k_fen_update<<<c->sm_count * 4, kThreads, 0, s>>>(c->g, c->d_owned, c->d_owned_count, c->d_mark, c->d_capr,
-                                                       c->d_lut, c->d_fen);
-    k_finalize<<<c->sm_count * 4, kThreads, 0, s>>>(c->d_owned, c->d_owned_count, c->d_mark, c->d_capr);
-    c->launches += 3;
+    const int grid = grid_for(c, v.n_nodes, 8);
+    int pi = prof_begin(c, s);
+    k_mark2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark, c->d_owner, c->d_status);
+    prof_end(c, s, pi, GR_K_MARK);
+    pi = prof_begin(c, s);
+    k_fen_update2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, c->d_mark, c->d_owner, c->d_capr,
+                                            c->d_lut, c->d_fen);
+    prof_end(c, s, pi, GR_K_FEN_UPDATE);
+    pi = prof_begin(c, s);
+    k_finalize2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, c->d_mark, c->d_owner, c->d_capr);
+    prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -319,7 +374,7 @@ const char *gr_error_string(int code) {
 }
 
 int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_cap) {
-    if (!out || !h_cap || X < 1 || Y < 1 || Z < 3) return GR_ERR_ARG;
+    if (!out || !h_cap || X < 1 || Y < 1 || Z < 3 || Z > kMaxLayers) return GR_ERR_ARG;
     int64_t csize = (int64_t)X * Y * Z;
     if (csize >= 0x7fffff00LL) return GR_ERR_ARG;  // cell ids are int32
     *out = nullptr;
@@ -345,8 +400,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
-        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owned, cell4) ||
-        cudaMalloc(&c->d_owned_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owner, cell4) || cudaMalloc(&c->d_status, 16) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -357,11 +411,11 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     c->h_cap0.assign(h_cap, h_cap + csize);
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
-        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_owned_count, 0, 16))
+        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16))
         return fail(GR_ERR_CUDA);
     c->mst_smem_max = (int)mst_smem(GR_MAX_PINS);
-    if (cudaFuncSetAttribute(k_mst, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
+        cudaSuccess)
         return fail(GR_ERR_CUDA);
     if ((rc = gr_reset(c, nullptr))) return fail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);
@@ -380,8 +434,7 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_lut);
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
-    cudaFree(c->d_owned);
-    cudaFree(c->d_owned_count);
+    cudaFree(c->d_owner);
     cudaFree(c->d_pins);
     free_buf(c->desc);
     free_buf(c->pcost);
@@ -390,6 +443,7 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->dist);
     free_buf(c->plan_desc);
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     if (c->stage_done) cudaEventDestroy(c->stage_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -401,8 +455,9 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
+    int pi = prof_begin(c, s);
     k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
-    c->launches++;
+    prof_end(c, s, pi, GR_K_FEN_INIT);
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -419,11 +474,15 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
         if (h_pins[t] < 0 || h_pins[t] >= c->csize) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
-    if (c->d_pins) cudaFree(c->d_pins);
-    c->d_pins = nullptr;
-    if (cudaMalloc(&c->d_pins, sizeof(int32_t) * (total + 1)) != cudaSuccess) {
-        cudaGetLastError();
-        return GR_ERR_NOMEM;
+    if ((size_t)(total + 1) > c->pins_cap) {
+        if (c->d_pins) cudaFree(c->d_pins);
+        c->d_pins = nullptr;
+        c->pins_cap = 0;
+        if (cudaMalloc(&c->d_pins, sizeof(int32_t) * (total + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return GR_ERR_NOMEM;
+        }
+        c->pins_cap = (size_t)(total + 1);
     }
     GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
     c->h_pin_ofs.assign(h_pin_ofs, h_pin_ofs + n_nets + 1);
@@ -437,9 +496,10 @@ int gr_lpattern(gr_ctx *c, const int32_t *d_pairs, int64_t n_pairs, float *d_cos
     if (!c || n_pairs < 0 || (n_pairs > 0 && (!d_pairs || !d_cost || !d_pat))) return GR_ERR_ARG;
     if (n_pairs == 0) return GR_OK;
     cudaStream_t s = pick(c, stream);
+    int pi = prof_begin(c, s);
     k_lpat_pairs<<<grid_for(c, n_pairs, 16), kThreads, 0, s>>>(c->g, (int)c->csize, d_pairs, n_pairs, c->d_fen,
                                                               d_cost, d_pat, c->d_status);
-    c->launches++;
+    prof_end(c, s, pi, GR_K_LPAT_PAIRS);
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -490,12 +550,22 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     GR_CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
     size_t bytes = desc_bytes(total > 0 ? total : 1);
-    std::vector<char> host(bytes);
+    if (bytes > c->h_stage_bytes) {
+        if (c->h_stage) GR_CK(cudaFreeHost(c->h_stage));
+        c->h_stage = nullptr;
+        c->h_stage_bytes = 0;
+        if (cudaMallocHost(&c->h_stage, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return GR_ERR_NOMEM;
+        }
+        c->h_stage_bytes = bytes;
+    }
+    char *host = (char *)c->h_stage;
     std::vector<BatchInfo> plan(n_batches);
     int64_t slot = 0, mp = 0, mt = 0, mn = 0;
     for (int32_t b = 0; b < n_batches; b++) {
         int rc = fill_desc(c, h_net_ids + h_batch_ofs[b], (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]),
-                           host.data(), total, h_batch_ofs[b], plan[b]);
+                           host, total, h_batch_ofs[b], plan[b]);
         if (rc) return rc;
         if ((rc = check_mst_smem(c, plan[b].max_pins))) return rc;
         plan[b].slot0 = slot;
@@ -506,7 +576,8 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     }
     int rc;
     if ((rc = ensure(c->plan_desc, bytes, c->stream))) return rc;
-    GR_CK(cudaMemcpyAsync(c->plan_desc.p, host.data(), bytes, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->plan_desc.p, host, bytes, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaEventRecord(c->stage_done, c->stream));
     if ((rc = ensure_scratch(c, mp, mt, mn, c->stream))) return rc;
     GR_CK(cudaStreamSynchronize(c->stream));
     c->plan = std::move(plan);
@@ -640,6 +711,43 @@ int gr_get_fenwick(gr_ctx *c, float *h_out) {
 }
 
 void *gr_stream(gr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int gr_profile_enable(gr_ctx *c, int on) {
+    if (!c) return GR_ERR_ARG;
+    c->profiling = on != 0;
+    return GR_OK;
+}
+
+int gr_profile_read(gr_ctx *c, double *ms, int64_t *launches, int reset) {
+    if (!c) return GR_ERR_ARG;
+    GR_CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i + 1 < c->ev_used; i += 2) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, c->ev[i], c->ev[i + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        int k = c->ev_kind[i / 2];
+        c->prof_ms[k] += t;
+        c->prof_n[k] += 1;
+    }
+    c->ev_used = 0;
+    for (int k = 0; k < GR_PROF_KINDS; k++) {
+        if (ms) ms[k] = c->prof_ms[k];
+        if (launches) launches[k] = c->prof_n[k];
+        if (reset) {
+            c->prof_ms[k] = 0;
+            c->prof_n[k] = 0;
+        }
+    }
+    return GR_OK;
+}
+
+const char *gr_kernel_name(int kind) {
+    static const char *names[GR_PROF_KINDS] = {"k_fen_init", "k_qtable", "k_lpat_batch", "k_mst", "k_mark",
+                                               "k_fen_update", "k_finalize", "k_lpat_pairs"};
+    return (kind >= 0 && kind < GR_PROF_KINDS) ? names[kind] : "";
+}
 
 int64_t gr_launch_count(gr_ctx *c) { return c ? c->launches : -1; }
 

@@ -19,6 +19,8 @@ constexpr int kLutMin = -256;  // cost LUT covers remaining capacity [-256, 1024
 constexpr int kLutMax = 1024;
 constexpr int kTableMaxPins = 1024;  // nets above this use direct Fenwick gathers
 constexpr int kMstMaxRounds = 40;
+constexpr int kMstWarpPins = 32;   // nets up to this size: one warp each
+constexpr int kMaxLayers = 32;     // layer sets are 64-bit masks
 
 struct GridC {
     int X, Y, Z, Z2, npat;

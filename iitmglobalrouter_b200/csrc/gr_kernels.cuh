@@ -1,12 +1,13 @@
 // gr_kernels.cuh -- kernels of the routing hot path (sm_100a).
 //
 // Per batch:
-//   k_qtable      per-net query tables (exact Fenwick prefix queries)
-//   k_lpat_batch  L-pattern argmin of every pin pair      (bit_util.hpp:119-191)
-//   k_mst         Boruvka spanning tree, one CTA per net   (gmst_util.hpp:164-341)
-//   k_mark        GCELLs of every MST edge, batch-deduped   (mst_bit_commit.hpp:81-235)
-//   k_fen_update  Fenwick node updates, one owner per node  (bit_util.hpp:75-90)
-//   k_finalize    demand += 1 per marked cell, marks cleared
+//   k_qtable       per-net query tables (exact Fenwick prefix queries)
+//   k_lpat_z<Z>    L-pattern argmin of every pin pair       (bit_util.hpp:119-191)
+//   k_mst_small    Boruvka, thread (2 pins) / warp (<= 32)   (gmst_util.hpp:164-341)
+//   k_mst_large    Boruvka, one CTA per larger net
+//   k_mark2        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_fen_update2  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_finalize2    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
 
@@ -183,7 +184,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total
 // larger root of each mutual pair -- computed here in parallel. A merged
 // component's root is its largest pin index (union points the smaller root at
 // the larger one), found by pointer jumping to each tree's top.
-__global__ void __launch_bounds__(256) k_mst(GridC g, BatchView bv, const float *__restrict__ cost,
+__global__ void __launch_bounds__(256) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                              int64_t *__restrict__ mst, float *__restrict__ dist,
                                              uint32_t *status) {
     extern __shared__ unsigned long long sm[];
@@ -203,14 +204,7 @@ __global__ void __launch_bounds__(256) k_mst(GridC g, BatchView bv, const float 
         const long long P = (long long)n * (n - 1) / 2;
         const float *w = cost + pofs;
         int64_t *out = mst + nofs;
-        if (n == 2) {  // one pair: edge (0,1), the reference's first candidate
-            if (tid == 0) {
-                out[0] = ((int64_t)net << 30) | 1;
-                out[1] = -1;
-                if (dist) dist[net] = w[0];
-            }
-            continue;
-        }
+        if (n <= kMstWarpPins) continue;  // k_mst_small's nets
         for (int v = tid; v < n; v += B) comp[v] = v;
         if (tid == 0) s_nrec = 0;
         float d = 0.0f;
@@ -278,8 +272,9 @@ __global__ void __launch_bounds__(256) k_mst(GridC g, BatchView bv, const float 
                 __syncthreads();
                 if (tid == 0) s_nrec += total;
             }
-            // tops of the candidate trees
-            while (true) {
+            // tops of the candidate trees (acyclic once mutual pairs are cut,
+            // so depth halves per step; the bound only guards the proof)
+            for (int step = 0;; step++) {
                 if (tid == 0) s_changed = 0;
                 __syncthreads();
                 for (int v = tid; v < n; v += B) {
@@ -291,6 +286,10 @@ __global__ void __launch_bounds__(256) k_mst(GridC g, BatchView bv, const float 
                 }
                 __syncthreads();
                 if (!s_changed) break;
+                if (step >= 64) {
+                    if (tid == 0) atomicOr(status, 0x4u);
+                    break;
+                }
                 __syncthreads();
             }
             for (int v = tid; v < n; v += B)
@@ -312,87 +311,340 @@ __global__ void __launch_bounds__(256) k_mst(GridC g, BatchView bv, const float 
     }
 }
 
+// ---------------------------------------------------------------- L-pattern, per-pair register tables
+// A pattern of pair (j -> k) only visits the pins' columns and the two
+// corners C1 = (x_k, y_j), C2 = (x_j, y_k). Per layer z the table entries at
+// (j,j), (k,k), (k,j), (j,k) give every query it makes:
+//   point costs  Pj, Pk, Pc1, Pc2     = Q(pos) - Q(pos-1) at J, K, C1, C2
+//   first wire   W1 (from J; even z along row y_j, odd z along column x_j)
+//   second wire  W2 (even z: row y_k from C2; odd z: column x_k from C1)
+// each the same single FP32 subtraction the reference's range query makes
+// (bit_util.hpp:36-38). With Z a compile-time constant the 6Z values stay
+// in registers and every pattern is summed in path order from them.
+template <int ZC>
+__device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int n, int j, int k, int z1, int z2, int xj,
+                                          int yj, int xk, int yk, float &out_c, int &out_p) {
+    constexpr int Z2 = (ZC + 1) / 2;
+    float Pj[ZC], Pk[ZC], Pc1[ZC], Pc2[ZC], W1[ZC], W2[ZC];
+    const int64_t nn = (int64_t)n * n;
+    const int ojj = j * n + j, okk = k * n + k, okj = k * n + j, ojk = j * n + k;
+    const bool xlt = xj < xk, ylt = yj < yk;
+    const bool mx = xj != xk, my = yj != yk;
+#pragma unroll
+    for (int z = 0; z < ZC; z++) {
+        const float2 *Tz = T + z * nn;
+        const float2 tjj = __ldg(Tz + ojj), tkk = __ldg(Tz + okk), tkj = __ldg(Tz + okj), tjk = __ldg(Tz + ojk);
+        Pj[z] = tjj.x - tjj.y;
+        Pk[z] = tkk.x - tkk.y;
+        Pc1[z] = tkj.x - tkj.y;
+        Pc2[z] = tjk.x - tjk.y;
+        if (z & 1) {
+            W1[z] = ylt ? tjk.x - tjj.y : tjj.x - tjk.y;  // column x_j, y_j -> y_k
+            W2[z] = ylt ? tkk.x - tkj.y : tkj.x - tkk.y;  // column x_k from C1
+        } else {
+            W1[z] = xlt ? tkj.x - tjj.y : tjj.x - tkj.y;  // row y_j, x_j -> x_k
+            W2[z] = xlt ? tkk.x - tjk.y : tjk.x - tkk.y;  // row y_k from C2
+        }
+    }
+    const bool bth = mx && my;
+    float best = __int_as_float(0x7f800000);
+    int bp = -1, first = -1;
+#pragma unroll
+    for (int via1 = 1; via1 < ZC; via1++) {
+        const bool even1 = (via1 & 1) == 0;
+        float c0 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < ZC; i++) {
+            const bool in = z1 < via1 ? (i >= z1 && i < via1) : (i >= via1 && i < z1);
+            if (in) c0 += Pj[i];
+        }
+        if (even1 ? mx : my) c0 += W1[via1];
+#pragma unroll
+        for (int v = 0; v < Z2; v++) {
+            const int cpat = via1 * Z2 + v;
+            const int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
+            float c = c0;
+            bool valid;
+            if (bth && via2 != 0) {
+                if (via2 >= ZC) continue;  // odd Z: no layer via2
+#pragma unroll
+                for (int i = 0; i < ZC; i++) {
+                    const bool in = (i >= (via1 < via2 ? via1 : via2)) && (i < (via1 < via2 ? via2 : via1));
+                    if (in) c += even1 ? Pc1[i] : Pc2[i];
+                }
+                c += W2[via2 < ZC ? via2 : 0];
+#pragma unroll
+                for (int i = 0; i < ZC; i++) {
+                    const bool in = via2 < z2 ? (i >= via2 && i < z2) : (i >= z2 && i < via2);
+                    if (in) c += Pk[i];
+                }
+                valid = true;
+            } else {
+#pragma unroll
+                for (int i = 0; i < ZC; i++) {
+                    const bool in = via1 < z2 ? (i >= via1 && i < z2) : (i >= z2 && i < via1);
+                    if (in) c += even1 ? Pc1[i] : Pc2[i];
+                }
+                valid = even1 ? !my : !mx;
+            }
+            if (!valid) continue;
+            if (first < 0) first = cpat;
+            if (c < best) {
+                best = c;
+                bp = cpat;
+            }
+        }
+    }
+    if (bp < 0) {
+        bp = first;
+        best = __int_as_float(0x7f800000);
+    }
+    out_c = best;
+    out_p = bp;
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                                const float *__restrict__ fen, const float2 *__restrict__ tab,
+                                                float *__restrict__ cost, int16_t *__restrict__ pat) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        const int net = ofs_search(bv.pair_ofs, bv.n, p);
+        const int n = bv.npin[net];
+        int j, k;
+        pair_decode(p - bv.pair_ofs[net], j, k);
+        const int32_t *np = pins + bv.pin_base[net];
+        int z1, x1, y1, z2, x2, y2;
+        dec(g, __ldg(np + j), z1, x1, y1);
+        dec(g, __ldg(np + k), z2, x2, y2);
+        float c;
+        int cp;
+        if (n <= kTableMaxPins) {
+            lpat_regs<ZC>(tab + bv.tab_ofs[net], n, j, k, z1, z2, x1, y1, x2, y2, c, cp);
+        } else {
+            DirectEv ev{fen, g, z1, x1, y1, z2, x2, y2, (x1 != x2 && y1 != y2)};
+            lpat_argmin(ev, g, c, cp);
+        }
+        cost[p] = c;
+        pat[p] = (int16_t)cp;
+    }
+}
+
+// ---------------------------------------------------------------- Boruvka, small nets
+// Nets of 2 pins: one thread each (the single pair is the tree; the
+// reference's first candidate root 0 records (0, 1)). Nets of 3..32 pins: one
+// warp each, pin = lane, the same per-round rule as k_mst_large with the
+// candidate forest resolved by shuffles.
+__global__ void __launch_bounds__(256) k_mst_small(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                   int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                   uint32_t *status) {
+    __shared__ unsigned long long skey[8][32];
+    __shared__ int scomp[8][32];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bv.n; i += gridDim.x * blockDim.x) {
+        if (bv.npin[i] != 2) continue;
+        const int64_t o = bv.node_ofs[i];
+        mst[o] = ((int64_t)i << 30) | 1;
+        mst[o + 1] = -1;
+        if (dist) dist[i] = cost[bv.pair_ofs[i]];
+    }
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + wib; i < bv.n; i += nwarps) {
+        const int n = bv.npin[i];
+        if (n < 3 || n > kMstWarpPins) continue;
+        const float *w = cost + bv.pair_ofs[i];
+        int64_t *out = mst + bv.node_ofs[i];
+        const int P = n * (n - 1) / 2;
+        scomp[wib][lane] = lane;
+        int nrec = 0;
+        float d = 0.0f;
+        for (int round = 0; nrec < n - 1 && round < kMstMaxRounds; round++) {
+            skey[wib][lane] = ~0ull;
+            __syncwarp();
+            int j, k;
+            pair_decode(lane, j, k);
+            for (int e = lane; e < P; e += 32) {
+                const int r1 = scomp[wib][j], r2 = scomp[wib][k];
+                if (r1 != r2) {
+                    const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
+                    atomicMin(&skey[wib][r1], kk);
+                    atomicMin(&skey[wib][r2], kk);
+                }
+                k += 32;
+                while (k >= j) {
+                    k -= j;
+                    j++;
+                }
+            }
+            __syncwarp();
+            int sel = -1;
+            const unsigned long long mykey = skey[wib][lane];
+            if (lane < n && scomp[wib][lane] == lane && mykey != ~0ull) {
+                int pj, pk;
+                pair_decode((long long)(uint32_t)mykey, pj, pk);
+                sel = scomp[wib][pj] == lane ? scomp[wib][pk] : scomp[wib][pj];
+            }
+            const int sel_of_sel = __shfl_sync(FULL, sel, sel < 0 ? 0 : sel);
+            const bool mutual_top = sel >= 0 && sel_of_sel == lane && lane > sel;
+            const bool rec = sel >= 0 && !mutual_top;
+            const unsigned recm = __ballot_sync(FULL, rec);
+            if (rec)
+                out[nrec + __popc(recm & ((1u << lane) - 1))] =
+                    ((int64_t)i << 30) | ((int64_t)lane << 15) | (int64_t)sel;
+            const float wv = rec ? __ldg(w + (uint32_t)mykey) : 0.0f;
+            for (int v = 0; v < 32; v++) {
+                const float t = __shfl_sync(FULL, wv, v);
+                if ((recm >> v) & 1u) d += t;
+            }
+            nrec += __popc(recm);
+            // tops of the candidate trees, then each tree's largest root
+            int par = sel >= 0 ? (mutual_top ? lane : sel) : lane;
+#pragma unroll
+            for (int it = 0; it < 5; it++) par = __shfl_sync(FULL, par, par);
+            const unsigned grp = __match_any_sync(FULL, sel >= 0 ? par : 64 + lane);
+            const int newroot = 31 - __clz(grp);
+            const int r_old = scomp[wib][lane];
+            const int sel_r = __shfl_sync(FULL, sel, r_old);
+            const int nr_r = __shfl_sync(FULL, newroot, r_old);
+            __syncwarp();
+            if (lane < n && sel_r >= 0) scomp[wib][lane] = nr_r;
+            __syncwarp();
+        }
+        for (int v = nrec + lane; v < n; v += 32) out[v] = -1;
+        if (lane == 0) {
+            if (dist) dist[i] = d;
+            if (nrec != n - 1) atomicOr(status, 0x4u);
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------- commit
-struct Marker {
+// The GCELLs of one committed edge (mst_bit_commit.hpp:36-67, 209-231): a
+// layer change covers its interior layers, a wire its inclusive span. Each
+// cell is visited once: V::span(first id, count) for a wire (ids contiguous
+// along the track), V::cell(id) for a via cell. Only stacked pins (same x
+// and y) can revisit a cell -- the two layer changes and the one-cell wire
+// share a column -- so that case visits the union of their layers.
+__device__ __forceinline__ uint64_t layer_interior(int a, int b) {
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    if (hi - lo < 2) return 0;
+    return ((1ull << hi) - 1) & ~((1ull << (lo + 1)) - 1);
+}
+
+template <class V>
+__device__ __forceinline__ bool walk_edge(const GridC &g, int z1, int x1, int y1, int z2, int x2, int y2, int cpat,
+                                          V &vis) {
+    const int via1 = cpat / g.Z2, v = cpat % g.Z2;
+    const bool bth = (x1 != x2 && y1 != y2);
+    const int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
+    if (cpat < 0 || via1 < 1 || via1 >= g.Z || (bth && via2 != 0 && via2 >= g.Z)) return false;
+    if (x1 == x2 && y1 == y2) {
+        uint64_t m = layer_interior(z1, via1) | (1ull << via1) | layer_interior(via1, z2);
+        while (m) {
+            const int i = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            vis.cell(enc(g, i, x1, y1));
+        }
+        return true;
+    }
+    auto via = [&](int za, int zb) {
+        const int lo = za < zb ? za : zb, hi = za < zb ? zb : za;
+        for (int i = lo + 1; i < hi; i++) vis.cell(enc(g, i, x1, y1));
+    };
+    auto wire = [&](int z) {
+        if (z & 1) {
+            const int lo = min(y1, y2), hi = max(y1, y2);
+            vis.span(z * g.XY + x1 * g.Y + lo, hi - lo + 1);
+            y1 = y2;
+        } else {
+            const int lo = min(x1, x2), hi = max(x1, x2);
+            vis.span(z * g.XY + y1 * g.X + lo, hi - lo + 1);
+            x1 = x2;
+        }
+    };
+    if (z1 != via1) {
+        via(z1, via1);
+        z1 = via1;
+    }
+    wire(z1);
+    if (bth && via2 != 0 && z1 != via2) {
+        via(z1, via2);
+        z1 = via2;
+        wire(z1);
+    }
+    if (z1 != z2) via(z1, z2);
+    return x1 == x2 && y1 == y2;
+}
+
+// decodes MST slot s of the batch; false for sentinels and invalid slots
+struct EdgeRef {
+    int net, cpat, z1, x1, y1, z2, x2, y2;
+};
+__device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, const int32_t *__restrict__ pins,
+                                       const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
+                                       int64_t s, EdgeRef &r) {
+    r.net = ofs_search(bv.node_ofs, bv.n, s);
+    const int64_t E = mst[s];
+    if (E == -1) return 0;
+    const int n = bv.npin[r.net];
+    int n1 = (int)(E & 0x7fff), n2 = (int)((E >> 15) & 0x7fff);
+    if ((E >> 30) != r.net || n1 >= n || n2 >= n || n1 == n2) return -1;
+    if (n1 < n2) {
+        const int t = n1;
+        n1 = n2;
+        n2 = t;
+    }
+    r.cpat = ppat[bv.pair_ofs[r.net] + (int64_t)n1 * (n1 - 1) / 2 + n2];
+    const int32_t *np = pins + bv.pin_base[r.net];
+    dec(g, __ldg(np + n1), r.z1, r.x1, r.y1);
+    dec(g, __ldg(np + n2), r.z2, r.x2, r.y2);
+    return 1;
+}
+
+// Marks with one atomicOr per bitmap word; the slot that sets a cell's bit
+// owns the cell for this batch.
+struct MarkVis {
     uint32_t *mark;
-    int32_t *owned;
-    int32_t *owned_count;
-    __device__ __forceinline__ void cell(int32_t e) const {
-        uint32_t bit = 1u << (e & 31);
-        uint32_t old = atomicOr(mark + (e >> 5), bit);
-        if (!(old & bit)) owned[atomicAdd(owned_count, 1)] = e;
+    int32_t *owner;
+    int32_t s;
+    __device__ __forceinline__ void span(int32_t e0, int cnt) {
+        const int32_t e1 = e0 + cnt - 1;
+        for (int w = e0 >> 5; w <= (e1 >> 5); w++) {
+            uint32_t m = 0xffffffffu;
+            if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
+            if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
+            uint32_t nb = m & ~atomicOr(mark + w, m);
+            while (nb) {
+                const int b = __ffs(nb) - 1;
+                nb &= nb - 1;
+                owner[(w << 5) + b] = s;
+            }
+        }
+    }
+    __device__ __forceinline__ void cell(int32_t e) {
+        const uint32_t bit = 1u << (e & 31);
+        if (!(atomicOr(mark + (e >> 5), bit) & bit)) owner[e] = s;
     }
 };
 
-// mst_bit_commit.hpp:36-67: a layer change marks its interior layers, a wire
-// marks its inclusive span.
-__device__ __forceinline__ void walk_via(const GridC &g, const Marker &m, int za, int zb, int x, int y) {
-    int zmin = za < zb ? za : zb, zmax = za < zb ? zb : za;
-    for (int i = zmin + 1; i < zmax; i++) m.cell(enc(g, i, x, y));
-}
-__device__ __forceinline__ void walk_wire(const GridC &g, const Marker &m, int z, int &x, int &y, int x2, int y2) {
-    if (z & 1) {
-        int lo = min(y, y2), hi = max(y, y2);
-        int32_t b = z * g.XY + x * g.Y;
-        for (int t = lo; t <= hi; t++) m.cell(b + t);
-        y = y2;
-    } else {
-        int lo = min(x, x2), hi = max(x, x2);
-        int32_t b = z * g.XY + y * g.X;
-        for (int t = lo; t <= hi; t++) m.cell(b + t);
-        x = x2;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_mark(GridC g, BatchView bv, const int32_t *__restrict__ pins,
-                                              const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                              int32_t *__restrict__ mst_pat, Marker m, uint32_t *status) {
+__global__ void __launch_bounds__(256) k_mark2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                               const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
+                                               int32_t *__restrict__ mst_pat, uint32_t *mark, int32_t *owner,
+                                               uint32_t *status) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
          s += (int64_t)gridDim.x * blockDim.x) {
-        int net = ofs_search(bv.node_ofs, bv.n, s);
-        int64_t E = mst[s];
-        if (E == -1) {
+        EdgeRef r;
+        const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
+        if (ok <= 0) {
             if (mst_pat) mst_pat[s] = -1;
+            if (ok < 0) atomicOr(status, 0x1u);
             continue;
         }
-        const int n = bv.npin[net];
-        int n1 = (int)(E & 0x7fff), n2 = (int)((E >> 15) & 0x7fff);
-        if ((E >> 30) != net || n1 >= n || n2 >= n || n1 == n2) {
-            atomicOr(status, 0x1u);
-            if (mst_pat) mst_pat[s] = -1;
-            continue;
-        }
-        if (n1 < n2) {
-            int t = n1;
-            n1 = n2;
-            n2 = t;
-        }
-        int cpat = ppat[bv.pair_ofs[net] + (int64_t)n1 * (n1 - 1) / 2 + n2];
-        if (mst_pat) mst_pat[s] = cpat;
-        const int32_t *np = pins + bv.pin_base[net];
-        int z1, x1, y1, z2, x2, y2;
-        dec(g, __ldg(np + n1), z1, x1, y1);
-        dec(g, __ldg(np + n2), z2, x2, y2);
-        int via1 = cpat / g.Z2, v = cpat % g.Z2;
-        bool bth = (x1 != x2 && y1 != y2);
-        int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
-        if (cpat < 0 || via1 < 1 || via1 >= g.Z || (bth && via2 != 0 && via2 >= g.Z)) {
-            atomicOr(status, 0x2u);
-            continue;
-        }
-        // mst_bit_commit.hpp:209-231
-        if (z1 != via1) {
-            walk_via(g, m, z1, via1, x1, y1);
-            z1 = via1;
-        }
-        walk_wire(g, m, z1, x1, y1, x2, y2);
-        if (bth && via2 != 0 && z1 != via2) {
-            walk_via(g, m, z1, via2, x1, y1);
-            z1 = via2;
-            walk_wire(g, m, z1, x1, y1, x2, y2);
-        }
-        if (z1 != z2) walk_via(g, m, z1, z2, x1, y1);
-        if (x1 != x2 || y1 != y2) atomicOr(status, 0x2u);
+        if (mst_pat) mst_pat[s] = r.cpat;
+        MarkVis vis{mark, owner, (int32_t)s};
+        if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
     }
 }
 
@@ -403,57 +655,102 @@ __device__ __forceinline__ uint32_t mark_word(const uint32_t *__restrict__ mark,
     return m;
 }
 
-// For each marked cell at track position p: walk its update path
+// For an owned cell at track position p: walk its update path
 // (bit_util.hpp:39-55). The cell owns node i while no other marked cell lies
 // in (p, i-1]; the owner adds the increments of every marked cell of the
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
-__global__ void __launch_bounds__(256) k_fen_update(GridC g, const int32_t *__restrict__ owned,
-                                                    const int32_t *__restrict__ owned_count,
-                                                    const uint32_t *__restrict__ mark,
-                                                    const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                    float *__restrict__ fen) {
-    const int cnt = *owned_count;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const int32_t e = owned[t];
-        int z, x, y;
-        dec(g, e, z, x, y);
-        const int p = (z & 1) ? y : x;
-        const int L = (z & 1) ? g.Y : g.X;
-        const int32_t base = e - p;
-        int32_t checked = e;  // no other marked cell in (e, checked]
-        for (int i = p + 1; i <= L; i += i & -i) {
-            const int32_t top = base + i - 1;
-            bool other = false;
-            for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
-                if (mark_word(mark, w, checked + 1, top)) {
-                    other = true;
-                    break;
-                }
-            if (other) break;
-            checked = top;
-            const int32_t lo = base + i - (i & -i);
-            float v = fen[top];
-            for (int w = lo >> 5; w <= (top >> 5); w++) {
-                uint32_t mw = mark_word(mark, w, lo, top);
-                while (mw) {
-                    int bit = __ffs(mw) - 1;
-                    mw &= mw - 1;
-                    v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
-                }
+__device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
+                                                 const int32_t *__restrict__ capr, const float *__restrict__ lut,
+                                                 float *__restrict__ fen) {
+    const int z = e / g.XY;
+    const int r = e - z * g.XY;
+    const int p = (z & 1) ? r % g.Y : r % g.X;
+    const int L = (z & 1) ? g.Y : g.X;
+    const int32_t base = e - p;
+    int32_t checked = e;  // no other marked cell in (e, checked]
+    for (int i = p + 1; i <= L; i += i & -i) {
+        const int32_t top = base + i - 1;
+        bool other = false;
+        for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
+            if (mark_word(mark, w, checked + 1, top)) {
+                other = true;
+                break;
             }
-            fen[top] = v;
+        if (other) break;
+        checked = top;
+        const int32_t lo = base + i - (i & -i);
+        float v = fen[top];
+        for (int w = lo >> 5; w <= (top >> 5); w++) {
+            uint32_t mw = mark_word(mark, w, lo, top);
+            while (mw) {
+                const int bit = __ffs(mw) - 1;
+                mw &= mw - 1;
+                v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
+            }
         }
+        fen[top] = v;
     }
 }
 
-__global__ void k_finalize(const int32_t *__restrict__ owned, const int32_t *__restrict__ owned_count,
-                           uint32_t *__restrict__ mark, int32_t *__restrict__ capr) {
-    const int cnt = *owned_count;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const int32_t e = owned[t];
-        capr[e] -= 1;
-        atomicAnd(mark + (e >> 5), ~(1u << (e & 31)));
+struct FenVis {
+    GridC g;
+    const uint32_t *mark;
+    const int32_t *owner;
+    const int32_t *capr;
+    const float *lut;
+    float *fen;
+    int32_t s;
+    __device__ __forceinline__ void cell(int32_t e) {
+        if (__ldg(owner + e) == s) fen_owner_update(g, e, mark, capr, lut, fen);
+    }
+    __device__ __forceinline__ void span(int32_t e0, int cnt) {
+        for (int t = 0; t < cnt; t++) cell(e0 + t);
+    }
+};
+
+__global__ void __launch_bounds__(256) k_fen_update2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                                     const int64_t *__restrict__ mst,
+                                                     const int16_t *__restrict__ ppat,
+                                                     const uint32_t *__restrict__ mark,
+                                                     const int32_t *__restrict__ owner,
+                                                     const int32_t *__restrict__ capr,
+                                                     const float *__restrict__ lut, float *__restrict__ fen) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        EdgeRef r;
+        if (edge_of(g, bv, pins, mst, ppat, s, r) <= 0) continue;
+        FenVis vis{g, mark, owner, capr, lut, fen, (int32_t)s};
+        walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis);
+    }
+}
+
+struct FinVis {
+    uint32_t *mark;
+    const int32_t *owner;
+    int32_t *capr;
+    int32_t s;
+    __device__ __forceinline__ void cell(int32_t e) {
+        if (owner[e] == s) {
+            capr[e] -= 1;
+            atomicAnd(mark + (e >> 5), ~(1u << (e & 31)));
+        }
+    }
+    __device__ __forceinline__ void span(int32_t e0, int cnt) {
+        for (int t = 0; t < cnt; t++) cell(e0 + t);
+    }
+};
+
+__global__ void __launch_bounds__(256) k_finalize2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                                   const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
+                                                   uint32_t *mark, const int32_t *__restrict__ owner,
+                                                   int32_t *__restrict__ capr) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        EdgeRef r;
+        if (edge_of(g, bv, pins, mst, ppat, s, r) <= 0) continue;
+        FinVis vis{mark, owner, capr, (int32_t)s};
+        walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis);
     }
 }
 

@@ -207,6 +207,19 @@ class Router:
                                              len(batch_ofs) - 1, ptr(batch_ofs), ptr(net_ids), ptr(mst_out),
                                              ptr(pat_out), 0), "gr_route_design_host")
 
+    # ---------------------------------------------------------- profiling
+    def profile(self, on: bool = True):
+        check(self._lib.gr_profile_enable(self._h, int(on)))
+
+    def profile_read(self, reset: bool = True) -> dict:
+        """{kernel name: (milliseconds, launches)} since the last reset."""
+        from ._capi import GR_PROF_KINDS
+        ms = np.zeros(GR_PROF_KINDS, dtype=np.float64)
+        n = np.zeros(GR_PROF_KINDS, dtype=np.int64)
+        check(self._lib.gr_profile_read(self._h, ptr(ms), ptr(n), int(reset)), "gr_profile_read")
+        return {self._lib.gr_kernel_name(k).decode(): (float(ms[k]), int(n[k])) for k in range(GR_PROF_KINDS)
+                if n[k]}
+
     # ---------------------------------------------------------- state
     def sync(self):
         check(self._lib.gr_sync(self._h), "gr_sync")

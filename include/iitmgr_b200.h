@@ -143,6 +143,23 @@ void *gr_stream(gr_ctx *ctx);                     /* the context's cudaStream_t 
 /* kernel launches issued by this context since creation (for accounting) */
 int64_t gr_launch_count(gr_ctx *ctx);
 
+/* Per-kernel timing: while enabled, every launch outside a graph capture is
+ * bracketed by CUDA events on its stream. gr_profile_read synchronises and
+ * returns, per kernel kind, the summed milliseconds and launch counts since
+ * the last reset. Costs an event pair per launch; off by default. */
+#define GR_K_FEN_INIT 0
+#define GR_K_QTABLE 1
+#define GR_K_LPAT 2
+#define GR_K_MST 3
+#define GR_K_MARK 4
+#define GR_K_FEN_UPDATE 5
+#define GR_K_FINALIZE 6
+#define GR_K_LPAT_PAIRS 7
+#define GR_PROF_KINDS 8
+int gr_profile_enable(gr_ctx *ctx, int on);
+int gr_profile_read(gr_ctx *ctx, double *ms, int64_t *launches, int reset);
+const char *gr_kernel_name(int kind);
+
 /* ------------------------------------------------------------ designs
  * Host-side design handling around the hot path (no GPU needed).
  * A gr_design holds the grid capacities and the multi-pin nets exactly as
