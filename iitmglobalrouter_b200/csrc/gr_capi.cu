@@ -35,6 +35,7 @@ struct BatchInfo {  // one batch of a plan
     int32_t n;
     int64_t n_pairs, n_nodes, n_tab, slot0;
     int32_t max_pins;
+    int32_t n2, nm, nl;  // nets of 2 pins, 3..32 pins, more
 };
 
 struct GraphCache {
@@ -56,7 +57,7 @@ struct gr_ctx {
     int32_t *d_cap0 = nullptr, *d_capr = nullptr;
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
-    int32_t *d_owner = nullptr;
+    int32_t *d_owner = nullptr, *d_owned = nullptr, *d_owned_count = nullptr;
     std::vector<int32_t> h_cap0;
     // design
     int32_t n_nets = 0;
@@ -156,7 +157,7 @@ int64_t tab_entries(const gr_ctx *c, int n) {
 }
 
 // bytes of a SoA descriptor of n nets
-size_t desc_bytes(int64_t n) { return (size_t)n * (sizeof(int32_t) + 4 * sizeof(int64_t)) + 64; }
+size_t desc_bytes(int64_t n) { return (size_t)n * (2 * sizeof(int32_t) + 4 * sizeof(int64_t)) + 64; }
 
 // lays the SoA arrays of n nets out in a buffer (int64 arrays first)
 BatchView view_of(void *buf, int64_t total_n, int64_t first, int32_t n) {
@@ -167,7 +168,9 @@ BatchView view_of(void *buf, int64_t total_n, int64_t first, int32_t n) {
     int64_t *node_ofs = pair_ofs + total_n;
     int64_t *tab_ofs = node_ofs + total_n;
     int32_t *npin = (int32_t *)(tab_ofs + total_n);
+    int32_t *order = npin + total_n;
     v.n = n;
+    v.order = order + first;
     v.npin = npin + first;
     v.pin_base = pin_base + first;
     v.pair_ofs = pair_ofs + first;
@@ -186,8 +189,9 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
     int64_t *node_ofs = const_cast<int64_t *>(v.node_ofs);
     int64_t *tab_ofs = const_cast<int64_t *>(v.tab_ofs);
     int32_t *npin = const_cast<int32_t *>(v.npin);
+    int32_t *order = const_cast<int32_t *>(v.order);
     int64_t P = 0, M = 0, T = 0;
-    int32_t mp = 0;
+    int32_t mp = 0, n2 = 0, nm = 0;
     for (int32_t i = 0; i < n; i++) {
         int32_t id = ids[i];
         if (id < 0 || id >= c->n_nets) return GR_ERR_ARG;
@@ -202,7 +206,18 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
         M += k;
         T += tab_entries(c, k);
         if (k > mp) mp = k;
+        n2 += k == 2;
+        nm += k > 2 && k <= kMstWarpPins;
     }
+    // nets by size class (k_mst_pin2 / k_mst_warp / k_mst_large), batch order kept
+    int32_t o2 = 0, om = n2, ol = n2 + nm;
+    for (int32_t i = 0; i < n; i++) {
+        const int32_t k = npin[i];
+        order[k == 2 ? o2++ : (k <= kMstWarpPins ? om++ : ol++)] = i;
+    }
+    bi.n2 = n2;
+    bi.nm = nm;
+    bi.nl = n - n2 - nm;
     bi.first = first;
     bi.n = n;
     bi.n_pairs = P;
@@ -218,6 +233,9 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
     v.n_nodes = bi.n_nodes;
     v.n_tab = bi.n_tab;
     v.max_pins = bi.max_pins;
+    v.n2 = bi.n2;
+    v.nm = bi.nm;
+    v.nl = bi.nl;
     return v;
 }
 
@@ -253,14 +271,21 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
 
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s) {
     if (v.n <= 0) return GR_OK;
-    int pi = prof_begin(c, s);
-    k_mst_small<<<grid_for(c, v.n, 8), kThreads, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
-    prof_end(c, s, pi, GR_K_MST);
-    if (v.max_pins > kMstWarpPins) {
+    if (v.n2 > 0) {
+        int pi = prof_begin(c, s);
+        k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
+        prof_end(c, s, pi, GR_K_MST);
+    }
+    if (v.nm > 0) {
+        int pi = prof_begin(c, s);
+        k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+        prof_end(c, s, pi, GR_K_MST);
+    }
+    if (v.nl > 0) {
         size_t sm = mst_smem(v.max_pins);
-        int blocks = v.n < c->sm_count * 8 ? v.n : c->sm_count * 8;
-        pi = prof_begin(c, s);
-        k_mst_large<<<blocks, kThreads, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+        int blocks = v.nl < c->sm_count * 4 ? v.nl : c->sm_count * 4;
+        int pi = prof_begin(c, s);
+        k_mst_large<<<blocks, 512, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s, pi, GR_K_MST);
     }
     GR_CK(cudaGetLastError());
@@ -270,16 +295,18 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
                   cudaStream_t s) {
     if (v.n_nodes <= 0) return GR_OK;
-    const int grid = grid_for(c, v.n_nodes, 8);
+    GR_CK(cudaMemsetAsync(c->d_owned_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
-    k_mark2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark, c->d_owner, c->d_status);
+    k_mark3<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
+                                                           c->d_owner, c->d_owned, c->d_owned_count, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, c->d_mark, c->d_owner, c->d_capr,
-                                            c->d_lut, c->d_fen);
+    k_fen_update3<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_owned, c->d_owned_count, c->d_mark, c->d_capr,
+                                                        c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
-    k_finalize2<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, c->d_mark, c->d_owner, c->d_capr);
+    k_finalize3<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_owned, c->d_owned_count, c->d_mark, c->d_owner,
+                                                      c->d_capr);
     prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -400,7 +427,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
-        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owner, cell4) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owner, cell4) || cudaMalloc(&c->d_owned, cell4) ||
+        cudaMalloc(&c->d_owned_count, 16) || cudaMalloc(&c->d_status, 16) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -411,7 +439,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     c->h_cap0.assign(h_cap, h_cap + csize);
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
-        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16))
+        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
+        cudaMemset(c->d_owned_count, 0, 16) || cudaMemset(c->d_owner, 0xff, cell4))
         return fail(GR_ERR_CUDA);
     c->mst_smem_max = (int)mst_smem(GR_MAX_PINS);
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
@@ -435,6 +464,8 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
     cudaFree(c->d_owner);
+    cudaFree(c->d_owned);
+    cudaFree(c->d_owned_count);
     cudaFree(c->d_pins);
     free_buf(c->desc);
     free_buf(c->pcost);
@@ -455,6 +486,7 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
+    GR_CK(cudaMemsetAsync(c->d_owner, 0xff, sizeof(int32_t) * (size_t)c->csize, s));
     int pi = prof_begin(c, s);
     k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_INIT);

@@ -3,11 +3,12 @@
 // Per batch:
 //   k_qtable       per-net query tables (exact Fenwick prefix queries)
 //   k_lpat_z<Z>    L-pattern argmin of every pin pair       (bit_util.hpp:119-191)
-//   k_mst_small    Boruvka, thread (2 pins) / warp (<= 32)   (gmst_util.hpp:164-341)
-//   k_mst_large    Boruvka, one CTA per larger net
-//   k_mark2        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update2  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize2    demand += 1 per marked cell, marks cleared
+//   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
+//   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
+//   k_mst_large    Boruvka of larger nets, one CTA each
+//   k_mark3        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_fen_update3  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_finalize3    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
 
@@ -22,8 +23,10 @@ struct BatchView {
     const int64_t *pair_ofs;  // [n] prefix of n(n-1)/2
     const int64_t *node_ofs;  // [n] prefix of n (MST slots)
     const int64_t *tab_ofs;   // [n] prefix of query-table entries
+    const int32_t *order;     // [n] net indices: 2-pin nets, then 3..32 pins, then larger
     int64_t n_pairs, n_nodes, n_tab;
     int32_t max_pins;
+    int32_t n2, nm, nl;       // sizes of the three classes in `order`
 };
 
 __device__ __forceinline__ float lut_cost(const float *__restrict__ lut, int c) {
@@ -184,9 +187,15 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total
 // larger root of each mutual pair -- computed here in parallel. A merged
 // component's root is its largest pin index (union points the smaller root at
 // the larger one), found by pointer jumping to each tree's top.
-__global__ void __launch_bounds__(256) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
-                                             int64_t *__restrict__ mst, float *__restrict__ dist,
-                                             uint32_t *status) {
+// Each pin scans its own pairs and posts one atomicMin to its root, so late
+// rounds (few components) see no atomic contention.
+__device__ __forceinline__ int64_t pair_id(int a, int b) {
+    return a > b ? (int64_t)a * (a - 1) / 2 + b : (int64_t)b * (b - 1) / 2 + a;
+}
+
+__global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                   int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                   uint32_t *status) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_nrec, s_changed;
@@ -198,13 +207,11 @@ __global__ void __launch_bounds__(256) k_mst_large(GridC g, BatchView bv, const 
     int *mx = par + maxn;
     int *flag = mx + maxn;
     const int B = blockDim.x, tid = threadIdx.x;
-    for (int net = blockIdx.x; net < bv.n; net += gridDim.x) {
+    for (int t = blockIdx.x; t < bv.nl; t += gridDim.x) {
+        const int net = bv.order[bv.n2 + bv.nm + t];
         const int n = bv.npin[net];
-        const int64_t pofs = bv.pair_ofs[net], nofs = bv.node_ofs[net];
-        const long long P = (long long)n * (n - 1) / 2;
-        const float *w = cost + pofs;
-        int64_t *out = mst + nofs;
-        if (n <= kMstWarpPins) continue;  // k_mst_small's nets
+        const float *w = cost + bv.pair_ofs[net];
+        int64_t *out = mst + bv.node_ofs[net];
         for (int v = tid; v < n; v += B) comp[v] = v;
         if (tid == 0) s_nrec = 0;
         float d = 0.0f;
@@ -214,22 +221,16 @@ __global__ void __launch_bounds__(256) k_mst_large(GridC g, BatchView bv, const 
             rounds++;
             for (int v = tid; v < n; v += B) key[v] = ~0ull;
             __syncthreads();
-            {
-                int j, k;
-                pair_decode(tid, j, k);
-                for (long long e = tid; e < P; e += B) {
-                    int r1 = comp[j], r2 = comp[k];
-                    if (r1 != r2) {
-                        unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
-                        atomicMin(key + r1, kk);
-                        atomicMin(key + r2, kk);
-                    }
-                    k += B;
-                    while (k >= j) {
-                        k -= j;
-                        j++;
-                    }
+            for (int v = tid; v < n; v += B) {
+                const int cv = comp[v];
+                unsigned long long best = ~0ull;
+                for (int u = 0; u < n; u++) {
+                    if (comp[u] == cv) continue;
+                    const int64_t e = pair_id(v, u);
+                    const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
+                    best = kk < best ? kk : best;
                 }
+                if (best != ~0ull) atomicMin(key + cv, best);
             }
             __syncthreads();
             for (int v = tid; v < n; v += B) {
@@ -432,91 +433,87 @@ __global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int
 
 // ---------------------------------------------------------------- Boruvka, small nets
 // Nets of 2 pins: one thread each (the single pair is the tree; the
-// reference's first candidate root 0 records (0, 1)). Nets of 3..32 pins: one
-// warp each, pin = lane, the same per-round rule as k_mst_large with the
-// candidate forest resolved by shuffles.
-__global__ void __launch_bounds__(256) k_mst_small(GridC g, BatchView bv, const float *__restrict__ cost,
-                                                   int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                   uint32_t *status) {
+// reference's first candidate root 0 records (0, 1)).
+__global__ void k_mst_pin2(BatchView bv, const float *__restrict__ cost, int64_t *__restrict__ mst,
+                           float *__restrict__ dist) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= bv.n2) return;
+    const int i = bv.order[t];
+    const int64_t o = bv.node_ofs[i];
+    mst[o] = ((int64_t)i << 30) | 1;
+    mst[o + 1] = -1;
+    if (dist) dist[i] = cost[bv.pair_ofs[i]];
+}
+
+// Nets of 3..32 pins: one warp each, pin = lane, the same per-round rule as
+// k_mst_large with the candidate forest resolved by shuffles.
+__global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                  int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                  uint32_t *status) {
     __shared__ unsigned long long skey[8][32];
     __shared__ int scomp[8][32];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < bv.n; i += gridDim.x * blockDim.x) {
-        if (bv.npin[i] != 2) continue;
-        const int64_t o = bv.node_ofs[i];
-        mst[o] = ((int64_t)i << 30) | 1;
-        mst[o + 1] = -1;
-        if (dist) dist[i] = cost[bv.pair_ofs[i]];
-    }
-    const int nwarps = gridDim.x * (blockDim.x >> 5);
-    for (int i = blockIdx.x * (blockDim.x >> 5) + wib; i < bv.n; i += nwarps) {
-        const int n = bv.npin[i];
-        if (n < 3 || n > kMstWarpPins) continue;
-        const float *w = cost + bv.pair_ofs[i];
-        int64_t *out = mst + bv.node_ofs[i];
-        const int P = n * (n - 1) / 2;
-        scomp[wib][lane] = lane;
-        int nrec = 0;
-        float d = 0.0f;
-        for (int round = 0; nrec < n - 1 && round < kMstMaxRounds; round++) {
-            skey[wib][lane] = ~0ull;
-            __syncwarp();
-            int j, k;
-            pair_decode(lane, j, k);
-            for (int e = lane; e < P; e += 32) {
-                const int r1 = scomp[wib][j], r2 = scomp[wib][k];
-                if (r1 != r2) {
-                    const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
-                    atomicMin(&skey[wib][r1], kk);
-                    atomicMin(&skey[wib][r2], kk);
-                }
-                k += 32;
-                while (k >= j) {
-                    k -= j;
-                    j++;
-                }
+    const int t = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (t >= bv.nm) return;
+    const int i = bv.order[bv.n2 + t];
+    const int n = bv.npin[i];
+    const float *w = cost + bv.pair_ofs[i];
+    int64_t *out = mst + bv.node_ofs[i];
+    scomp[wib][lane] = lane;
+    int nrec = 0;
+    float d = 0.0f;
+    for (int round = 0; nrec < n - 1 && round < kMstMaxRounds; round++) {
+        skey[wib][lane] = ~0ull;
+        __syncwarp();
+        if (lane < n) {
+            const int cv = scomp[wib][lane];
+            unsigned long long best = ~0ull;
+            for (int u = 0; u < n; u++) {
+                if (scomp[wib][u] == cv) continue;
+                const int64_t e = pair_id(lane, u);
+                const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
+                best = kk < best ? kk : best;
             }
-            __syncwarp();
-            int sel = -1;
-            const unsigned long long mykey = skey[wib][lane];
-            if (lane < n && scomp[wib][lane] == lane && mykey != ~0ull) {
-                int pj, pk;
-                pair_decode((long long)(uint32_t)mykey, pj, pk);
-                sel = scomp[wib][pj] == lane ? scomp[wib][pk] : scomp[wib][pj];
-            }
-            const int sel_of_sel = __shfl_sync(FULL, sel, sel < 0 ? 0 : sel);
-            const bool mutual_top = sel >= 0 && sel_of_sel == lane && lane > sel;
-            const bool rec = sel >= 0 && !mutual_top;
-            const unsigned recm = __ballot_sync(FULL, rec);
-            if (rec)
-                out[nrec + __popc(recm & ((1u << lane) - 1))] =
-                    ((int64_t)i << 30) | ((int64_t)lane << 15) | (int64_t)sel;
-            const float wv = rec ? __ldg(w + (uint32_t)mykey) : 0.0f;
-            for (int v = 0; v < 32; v++) {
-                const float t = __shfl_sync(FULL, wv, v);
-                if ((recm >> v) & 1u) d += t;
-            }
-            nrec += __popc(recm);
-            // tops of the candidate trees, then each tree's largest root
-            int par = sel >= 0 ? (mutual_top ? lane : sel) : lane;
-#pragma unroll
-            for (int it = 0; it < 5; it++) par = __shfl_sync(FULL, par, par);
-            const unsigned grp = __match_any_sync(FULL, sel >= 0 ? par : 64 + lane);
-            const int newroot = 31 - __clz(grp);
-            const int r_old = scomp[wib][lane];
-            const int sel_r = __shfl_sync(FULL, sel, r_old);
-            const int nr_r = __shfl_sync(FULL, newroot, r_old);
-            __syncwarp();
-            if (lane < n && sel_r >= 0) scomp[wib][lane] = nr_r;
-            __syncwarp();
-        }
-        for (int v = nrec + lane; v < n; v += 32) out[v] = -1;
-        if (lane == 0) {
-            if (dist) dist[i] = d;
-            if (nrec != n - 1) atomicOr(status, 0x4u);
+            if (best != ~0ull) atomicMin(&skey[wib][cv], best);
         }
         __syncwarp();
+        int sel = -1;
+        const unsigned long long mykey = skey[wib][lane];
+        if (lane < n && scomp[wib][lane] == lane && mykey != ~0ull) {
+            int pj, pk;
+            pair_decode((long long)(uint32_t)mykey, pj, pk);
+            sel = scomp[wib][pj] == lane ? scomp[wib][pk] : scomp[wib][pj];
+        }
+        const int sel_of_sel = __shfl_sync(FULL, sel, sel < 0 ? 0 : sel);
+        const bool mutual_top = sel >= 0 && sel_of_sel == lane && lane > sel;
+        const bool rec = sel >= 0 && !mutual_top;
+        const unsigned recm = __ballot_sync(FULL, rec);
+        if (rec)
+            out[nrec + __popc(recm & ((1u << lane) - 1))] = ((int64_t)i << 30) | ((int64_t)lane << 15) | (int64_t)sel;
+        const float wv = rec ? __ldg(w + (uint32_t)mykey) : 0.0f;
+        for (int v = 0; v < 32; v++) {
+            const float x = __shfl_sync(FULL, wv, v);
+            if ((recm >> v) & 1u) d += x;
+        }
+        nrec += __popc(recm);
+        // tops of the candidate trees, then each tree's largest root
+        int par = sel >= 0 ? (mutual_top ? lane : sel) : lane;
+#pragma unroll
+        for (int it = 0; it < 5; it++) par = __shfl_sync(FULL, par, par);
+        const unsigned grp = __match_any_sync(FULL, sel >= 0 ? par : 64 + lane);
+        const int newroot = 31 - __clz(grp);
+        const int r_old = scomp[wib][lane];
+        const int sel_r = __shfl_sync(FULL, sel, r_old);
+        const int nr_r = __shfl_sync(FULL, newroot, r_old);
+        __syncwarp();
+        if (lane < n && sel_r >= 0) scomp[wib][lane] = nr_r;
+        __syncwarp();
+    }
+    for (int v = nrec + lane; v < n; v += 32) out[v] = -1;
+    if (lane == 0) {
+        if (dist) dist[i] = d;
+        if (nrec != n - 1) atomicOr(status, 0x4u);
     }
 }
 
@@ -604,18 +601,20 @@ __device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, cons
 }
 
 // Marks with one atomicOr per bitmap word; the slot that sets a cell's bit
-// owns the cell for this batch.
+// owns the cell for this batch (owner entries are -1 outside a batch).
 struct MarkVis {
     uint32_t *mark;
     int32_t *owner;
     int32_t s;
-    __device__ __forceinline__ void span(int32_t e0, int cnt) {
-        const int32_t e1 = e0 + cnt - 1;
+    int cnt;
+    __device__ __forceinline__ void span(int32_t e0, int n) {
+        const int32_t e1 = e0 + n - 1;
         for (int w = e0 >> 5; w <= (e1 >> 5); w++) {
             uint32_t m = 0xffffffffu;
             if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
             if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
             uint32_t nb = m & ~atomicOr(mark + w, m);
+            cnt += __popc(nb);
             while (nb) {
                 const int b = __ffs(nb) - 1;
                 nb &= nb - 1;
@@ -625,26 +624,64 @@ struct MarkVis {
     }
     __device__ __forceinline__ void cell(int32_t e) {
         const uint32_t bit = 1u << (e & 31);
-        if (!(atomicOr(mark + (e >> 5), bit) & bit)) owner[e] = s;
+        if (!(atomicOr(mark + (e >> 5), bit) & bit)) {
+            owner[e] = s;
+            cnt++;
+        }
     }
 };
 
-__global__ void __launch_bounds__(256) k_mark2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+// Appends the cells this slot owns (owner == s) to the batch's list.
+struct EmitVis {
+    const int32_t *owner;
+    int32_t *list;
+    int32_t s;
+    int64_t at;
+    __device__ __forceinline__ void cell(int32_t e) {
+        if (owner[e] == s) list[at++] = e;
+    }
+    __device__ __forceinline__ void span(int32_t e0, int n) {
+        for (int t = 0; t < n; t++) cell(e0 + t);
+    }
+};
+
+// One thread per MST slot: mark the edge's GCELLs, then (after a block scan
+// of the per-thread counts and one global atomic per block) list the cells
+// it owns.
+__global__ void __launch_bounds__(256) k_mark3(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
                                                int32_t *__restrict__ mst_pat, uint32_t *mark, int32_t *owner,
+                                               int32_t *__restrict__ owned, int32_t *owned_count,
                                                uint32_t *status) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
-         s += (int64_t)gridDim.x * blockDim.x) {
+    __shared__ int warp_sums[32];
+    __shared__ int s_base;
+    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x; s0 < bv.n_nodes; s0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = s0 + threadIdx.x;
         EdgeRef r;
-        const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
-        if (ok <= 0) {
-            if (mst_pat) mst_pat[s] = -1;
-            if (ok < 0) atomicOr(status, 0x1u);
-            continue;
+        int cnt = 0;
+        bool have = false;
+        if (s < bv.n_nodes) {
+            const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
+            if (ok <= 0) {
+                if (mst_pat) mst_pat[s] = -1;
+                if (ok < 0) atomicOr(status, 0x1u);
+            } else {
+                if (mst_pat) mst_pat[s] = r.cpat;
+                MarkVis vis{mark, owner, (int32_t)s, 0};
+                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
+                cnt = vis.cnt;
+                have = true;
+            }
         }
-        if (mst_pat) mst_pat[s] = r.cpat;
-        MarkVis vis{mark, owner, (int32_t)s};
-        if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
+        int total;
+        const int pre = block_excl_scan(cnt, warp_sums, total);
+        if (threadIdx.x == 0) s_base = total ? atomicAdd(owned_count, total) : 0;
+        __syncthreads();
+        if (have && cnt) {
+            EmitVis em{owner, owned, (int32_t)s, (int64_t)s_base + pre};
+            walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, em);
+        }
+        __syncthreads();
     }
 }
 
@@ -655,102 +692,59 @@ __device__ __forceinline__ uint32_t mark_word(const uint32_t *__restrict__ mark,
     return m;
 }
 
-// For an owned cell at track position p: walk its update path
+// For each marked cell at track position p: walk its update path
 // (bit_util.hpp:39-55). The cell owns node i while no other marked cell lies
 // in (p, i-1]; the owner adds the increments of every marked cell of the
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
-__device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
-                                                 const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                 float *__restrict__ fen) {
-    const int z = e / g.XY;
-    const int r = e - z * g.XY;
-    const int p = (z & 1) ? r % g.Y : r % g.X;
-    const int L = (z & 1) ? g.Y : g.X;
-    const int32_t base = e - p;
-    int32_t checked = e;  // no other marked cell in (e, checked]
-    for (int i = p + 1; i <= L; i += i & -i) {
-        const int32_t top = base + i - 1;
-        bool other = false;
-        for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
-            if (mark_word(mark, w, checked + 1, top)) {
-                other = true;
-                break;
-            }
-        if (other) break;
-        checked = top;
-        const int32_t lo = base + i - (i & -i);
-        float v = fen[top];
-        for (int w = lo >> 5; w <= (top >> 5); w++) {
-            uint32_t mw = mark_word(mark, w, lo, top);
-            while (mw) {
-                const int bit = __ffs(mw) - 1;
-                mw &= mw - 1;
-                v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
-            }
-        }
-        fen[top] = v;
-    }
-}
-
-struct FenVis {
-    GridC g;
-    const uint32_t *mark;
-    const int32_t *owner;
-    const int32_t *capr;
-    const float *lut;
-    float *fen;
-    int32_t s;
-    __device__ __forceinline__ void cell(int32_t e) {
-        if (__ldg(owner + e) == s) fen_owner_update(g, e, mark, capr, lut, fen);
-    }
-    __device__ __forceinline__ void span(int32_t e0, int cnt) {
-        for (int t = 0; t < cnt; t++) cell(e0 + t);
-    }
-};
-
-__global__ void __launch_bounds__(256) k_fen_update2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
-                                                     const int64_t *__restrict__ mst,
-                                                     const int16_t *__restrict__ ppat,
+__global__ void __launch_bounds__(256) k_fen_update3(GridC g, const int32_t *__restrict__ owned,
+                                                     const int32_t *__restrict__ owned_count,
                                                      const uint32_t *__restrict__ mark,
-                                                     const int32_t *__restrict__ owner,
-                                                     const int32_t *__restrict__ capr,
-                                                     const float *__restrict__ lut, float *__restrict__ fen) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        EdgeRef r;
-        if (edge_of(g, bv, pins, mst, ppat, s, r) <= 0) continue;
-        FenVis vis{g, mark, owner, capr, lut, fen, (int32_t)s};
-        walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis);
+                                                     const int32_t *__restrict__ capr, const float *__restrict__ lut,
+                                                     float *__restrict__ fen) {
+    const int cnt = *owned_count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const int32_t e = owned[t];
+        const int z = e / g.XY;
+        const int r = e - z * g.XY;
+        const int p = (z & 1) ? r % g.Y : r % g.X;
+        const int L = (z & 1) ? g.Y : g.X;
+        const int32_t base = e - p;
+        int32_t checked = e;  // no other marked cell in (e, checked]
+        for (int i = p + 1; i <= L; i += i & -i) {
+            const int32_t top = base + i - 1;
+            bool other = false;
+            for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
+                if (mark_word(mark, w, checked + 1, top)) {
+                    other = true;
+                    break;
+                }
+            if (other) break;
+            checked = top;
+            const int32_t lo = base + i - (i & -i);
+            float v = fen[top];
+            for (int w = lo >> 5; w <= (top >> 5); w++) {
+                uint32_t mw = mark_word(mark, w, lo, top);
+                while (mw) {
+                    const int bit = __ffs(mw) - 1;
+                    mw &= mw - 1;
+                    v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
+                }
+            }
+            fen[top] = v;
+        }
     }
 }
 
-struct FinVis {
-    uint32_t *mark;
-    const int32_t *owner;
-    int32_t *capr;
-    int32_t s;
-    __device__ __forceinline__ void cell(int32_t e) {
-        if (owner[e] == s) {
-            capr[e] -= 1;
-            atomicAnd(mark + (e >> 5), ~(1u << (e & 31)));
-        }
-    }
-    __device__ __forceinline__ void span(int32_t e0, int cnt) {
-        for (int t = 0; t < cnt; t++) cell(e0 + t);
-    }
-};
-
-__global__ void __launch_bounds__(256) k_finalize2(GridC g, BatchView bv, const int32_t *__restrict__ pins,
-                                                   const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                                   uint32_t *mark, const int32_t *__restrict__ owner,
-                                                   int32_t *__restrict__ capr) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        EdgeRef r;
-        if (edge_of(g, bv, pins, mst, ppat, s, r) <= 0) continue;
-        FinVis vis{mark, owner, capr, (int32_t)s};
-        walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis);
+// demand += 1 for every marked cell; marks and owners cleared for the next batch
+__global__ void k_finalize3(const int32_t *__restrict__ owned, const int32_t *__restrict__ owned_count,
+                            uint32_t *__restrict__ mark, int32_t *__restrict__ owner, int32_t *__restrict__ capr) {
+    const int cnt = *owned_count;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+        const int32_t e = owned[t];
+        capr[e] -= 1;
+        owner[e] = -1;
+        atomicAnd(mark + (e >> 5), ~(1u << (e & 31)));
     }
 }
 
