@@ -57,7 +57,8 @@ struct gr_ctx {
     int32_t *d_cap0 = nullptr, *d_capr = nullptr;
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
-    int32_t *d_owner = nullptr, *d_owned = nullptr, *d_owned_count = nullptr;
+    unsigned long long *d_list = nullptr;  // (word, newly set bits) of a batch's marked cells
+    int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
     // design
     int32_t n_nets = 0;
@@ -89,6 +90,7 @@ struct gr_ctx {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
 
 #define GR_CK(call)                                                                            \
     do {                                                                                       \
@@ -282,10 +284,15 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         prof_end(c, s, pi, GR_K_MST);
     }
     if (v.nl > 0) {
-        size_t sm = mst_smem(v.max_pins);
+        // stage the pair costs of a net in shared memory when they fit
+        const int64_t maxp = (int64_t)v.max_pins * (v.max_pins - 1) / 2;
+        const size_t base = mst_smem(v.max_pins);
+        const int64_t room = ((int64_t)kMstSmemMax - (int64_t)base) / 4;
+        const int64_t stage = maxp < room ? maxp : room;  // nets with at most `stage` pairs are staged
+        const size_t sm = base + (size_t)stage * 4;
         int blocks = v.nl < c->sm_count * 4 ? v.nl : c->sm_count * 4;
         int pi = prof_begin(c, s);
-        k_mst_large<<<blocks, 512, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status);
+        k_mst_large<<<blocks, 512, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status, stage);
         prof_end(c, s, pi, GR_K_MST);
     }
     GR_CK(cudaGetLastError());
@@ -295,18 +302,17 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
                   cudaStream_t s) {
     if (v.n_nodes <= 0) return GR_OK;
-    GR_CK(cudaMemsetAsync(c->d_owned_count, 0, sizeof(int32_t), s));
+    GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
-    k_mark3<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                           c->d_owner, c->d_owned, c->d_owned_count, c->d_status);
+    k_mark4<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
+                                                           c->d_list, c->d_list_count, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update3<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_owned, c->d_owned_count, c->d_mark, c->d_capr,
+    k_fen_update4<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_capr,
                                                         c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
-    k_finalize3<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_owned, c->d_owned_count, c->d_mark, c->d_owner,
-                                                      c->d_capr);
+    k_finalize4<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_capr);
     prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -427,8 +433,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
-        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_owner, cell4) || cudaMalloc(&c->d_owned, cell4) ||
-        cudaMalloc(&c->d_owned_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list, sizeof(unsigned long long) * (size_t)csize) ||
+        cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -440,9 +446,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
         cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_owned_count, 0, 16) || cudaMemset(c->d_owner, 0xff, cell4))
+        cudaMemset(c->d_list_count, 0, 16))
         return fail(GR_ERR_CUDA);
-    c->mst_smem_max = (int)mst_smem(GR_MAX_PINS);
+    c->mst_smem_max = kMstSmemMax;
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
         cudaSuccess)
         return fail(GR_ERR_CUDA);
@@ -463,9 +469,8 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_lut);
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
-    cudaFree(c->d_owner);
-    cudaFree(c->d_owned);
-    cudaFree(c->d_owned_count);
+    cudaFree(c->d_list);
+    cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
     free_buf(c->desc);
     free_buf(c->pcost);
@@ -486,7 +491,6 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
-    GR_CK(cudaMemsetAsync(c->d_owner, 0xff, sizeof(int32_t) * (size_t)c->csize, s));
     int pi = prof_begin(c, s);
     k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_INIT);

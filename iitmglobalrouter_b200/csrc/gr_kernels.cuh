@@ -6,9 +6,9 @@
 //   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
-//   k_mark3        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update3  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize3    demand += 1 per marked cell, marks cleared
+//   k_mark4        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_fen_update4  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_finalize4    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
 
@@ -195,7 +195,7 @@ __device__ __forceinline__ int64_t pair_id(int a, int b) {
 
 __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                   uint32_t *status) {
+                                                   uint32_t *status, int64_t stage_pairs) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_nrec, s_changed;
@@ -207,10 +207,16 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
     int *mx = par + maxn;
     int *flag = mx + maxn;
     const int B = blockDim.x, tid = threadIdx.x;
+    float *wsm = (float *)(flag + maxn);  // pair costs, when the net's fit
     for (int t = blockIdx.x; t < bv.nl; t += gridDim.x) {
         const int net = bv.order[bv.n2 + bv.nm + t];
         const int n = bv.npin[net];
+        const int64_t P = (int64_t)n * (n - 1) / 2;
         const float *w = cost + bv.pair_ofs[net];
+        if (P <= stage_pairs) {
+            for (int64_t e = tid; e < P; e += B) wsm[e] = __ldg(w + e);
+            w = wsm;
+        }
         int64_t *out = mst + bv.node_ofs[net];
         for (int v = tid; v < n; v += B) comp[v] = v;
         if (tid == 0) s_nrec = 0;
@@ -227,7 +233,7 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
                 for (int u = 0; u < n; u++) {
                     if (comp[u] == cv) continue;
                     const int64_t e = pair_id(v, u);
-                    const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
+                    const unsigned long long kk = cost_key(w[e], (uint32_t)e);
                     best = kk < best ? kk : best;
                 }
                 if (best != ~0ull) atomicMin(key + cv, best);
@@ -452,13 +458,19 @@ __global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const f
                                                   uint32_t *status) {
     __shared__ unsigned long long skey[8][32];
     __shared__ int scomp[8][32];
+    __shared__ float sw[8][kMstWarpPins * (kMstWarpPins - 1) / 2];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int t = blockIdx.x * (blockDim.x >> 5) + wib;
     if (t >= bv.nm) return;
     const int i = bv.order[bv.n2 + t];
     const int n = bv.npin[i];
-    const float *w = cost + bv.pair_ofs[i];
+    {
+        const float *wg = cost + bv.pair_ofs[i];
+        for (int e = lane; e < n * (n - 1) / 2; e += 32) sw[wib][e] = __ldg(wg + e);
+        __syncwarp();
+    }
+    const float *w = sw[wib];
     int64_t *out = mst + bv.node_ofs[i];
     scomp[wib][lane] = lane;
     int nrec = 0;
@@ -472,7 +484,7 @@ __global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const f
             for (int u = 0; u < n; u++) {
                 if (scomp[wib][u] == cv) continue;
                 const int64_t e = pair_id(lane, u);
-                const unsigned long long kk = cost_key(__ldg(w + e), (uint32_t)e);
+                const unsigned long long kk = cost_key(w[e], (uint32_t)e);
                 best = kk < best ? kk : best;
             }
             if (best != ~0ull) atomicMin(&skey[wib][cv], best);
@@ -491,7 +503,7 @@ __global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const f
         const unsigned recm = __ballot_sync(FULL, rec);
         if (rec)
             out[nrec + __popc(recm & ((1u << lane) - 1))] = ((int64_t)i << 30) | ((int64_t)lane << 15) | (int64_t)sel;
-        const float wv = rec ? __ldg(w + (uint32_t)mykey) : 0.0f;
+        const float wv = rec ? w[(uint32_t)mykey] : 0.0f;
         for (int v = 0; v < 32; v++) {
             const float x = __shfl_sync(FULL, wv, v);
             if ((recm >> v) & 1u) d += x;
@@ -600,88 +612,57 @@ __device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, cons
     return 1;
 }
 
-// Marks with one atomicOr per bitmap word; the slot that sets a cell's bit
-// owns the cell for this batch (owner entries are -1 outside a batch).
+// Marks with one atomicOr per bitmap word. The bits a slot sets first are
+// the cells it owns for this batch; each (word, newly set bits) pair is
+// appended to the batch's list with one warp-aggregated atomic.
+__device__ __forceinline__ void list_append(unsigned long long *list, int32_t *count, int32_t w, uint32_t bits) {
+    const unsigned active = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(active) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(active));
+    base = __shfl_sync(active, base, leader);
+    list[base + __popc(active & ((1u << lane) - 1))] = ((unsigned long long)(uint32_t)w << 32) | bits;
+}
+
 struct MarkVis {
     uint32_t *mark;
-    int32_t *owner;
-    int32_t s;
-    int cnt;
+    unsigned long long *list;
+    int32_t *count;
     __device__ __forceinline__ void span(int32_t e0, int n) {
         const int32_t e1 = e0 + n - 1;
         for (int w = e0 >> 5; w <= (e1 >> 5); w++) {
             uint32_t m = 0xffffffffu;
             if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
             if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
-            uint32_t nb = m & ~atomicOr(mark + w, m);
-            cnt += __popc(nb);
-            while (nb) {
-                const int b = __ffs(nb) - 1;
-                nb &= nb - 1;
-                owner[(w << 5) + b] = s;
-            }
+            const uint32_t nb = m & ~atomicOr(mark + w, m);
+            if (nb) list_append(list, count, w, nb);
         }
     }
     __device__ __forceinline__ void cell(int32_t e) {
         const uint32_t bit = 1u << (e & 31);
-        if (!(atomicOr(mark + (e >> 5), bit) & bit)) {
-            owner[e] = s;
-            cnt++;
-        }
+        if (!(atomicOr(mark + (e >> 5), bit) & bit)) list_append(list, count, e >> 5, bit);
     }
 };
 
-// Appends the cells this slot owns (owner == s) to the batch's list.
-struct EmitVis {
-    const int32_t *owner;
-    int32_t *list;
-    int32_t s;
-    int64_t at;
-    __device__ __forceinline__ void cell(int32_t e) {
-        if (owner[e] == s) list[at++] = e;
-    }
-    __device__ __forceinline__ void span(int32_t e0, int n) {
-        for (int t = 0; t < n; t++) cell(e0 + t);
-    }
-};
-
-// One thread per MST slot: mark the edge's GCELLs, then (after a block scan
-// of the per-thread counts and one global atomic per block) list the cells
-// it owns.
-__global__ void __launch_bounds__(256) k_mark3(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+// One thread per MST slot: mark the GCELLs of its edge.
+__global__ void __launch_bounds__(256) k_mark4(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                               int32_t *__restrict__ mst_pat, uint32_t *mark, int32_t *owner,
-                                               int32_t *__restrict__ owned, int32_t *owned_count,
+                                               int32_t *__restrict__ mst_pat, uint32_t *mark,
+                                               unsigned long long *__restrict__ list, int32_t *count,
                                                uint32_t *status) {
-    __shared__ int warp_sums[32];
-    __shared__ int s_base;
-    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x; s0 < bv.n_nodes; s0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t s = s0 + threadIdx.x;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
+         s += (int64_t)gridDim.x * blockDim.x) {
         EdgeRef r;
-        int cnt = 0;
-        bool have = false;
-        if (s < bv.n_nodes) {
-            const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
-            if (ok <= 0) {
-                if (mst_pat) mst_pat[s] = -1;
-                if (ok < 0) atomicOr(status, 0x1u);
-            } else {
-                if (mst_pat) mst_pat[s] = r.cpat;
-                MarkVis vis{mark, owner, (int32_t)s, 0};
-                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
-                cnt = vis.cnt;
-                have = true;
-            }
+        const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
+        if (ok <= 0) {
+            if (mst_pat) mst_pat[s] = -1;
+            if (ok < 0) atomicOr(status, 0x1u);
+            continue;
         }
-        int total;
-        const int pre = block_excl_scan(cnt, warp_sums, total);
-        if (threadIdx.x == 0) s_base = total ? atomicAdd(owned_count, total) : 0;
-        __syncthreads();
-        if (have && cnt) {
-            EmitVis em{owner, owned, (int32_t)s, (int64_t)s_base + pre};
-            walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, em);
-        }
-        __syncthreads();
+        if (mst_pat) mst_pat[s] = r.cpat;
+        MarkVis vis{mark, list, count};
+        if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
     }
 }
 
@@ -692,59 +673,77 @@ __device__ __forceinline__ uint32_t mark_word(const uint32_t *__restrict__ mark,
     return m;
 }
 
-// For each marked cell at track position p: walk its update path
+// For a marked cell at track position p: walk its update path
 // (bit_util.hpp:39-55). The cell owns node i while no other marked cell lies
 // in (p, i-1]; the owner adds the increments of every marked cell of the
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
-__global__ void __launch_bounds__(256) k_fen_update3(GridC g, const int32_t *__restrict__ owned,
-                                                     const int32_t *__restrict__ owned_count,
+__device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
+                                                 const int32_t *__restrict__ capr, const float *__restrict__ lut,
+                                                 float *__restrict__ fen) {
+    const int z = e / g.XY;
+    const int r = e - z * g.XY;
+    const int p = (z & 1) ? r % g.Y : r % g.X;
+    const int L = (z & 1) ? g.Y : g.X;
+    const int32_t base = e - p;
+    int32_t checked = e;  // no other marked cell in (e, checked]
+    for (int i = p + 1; i <= L; i += i & -i) {
+        const int32_t top = base + i - 1;
+        bool other = false;
+        for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
+            if (mark_word(mark, w, checked + 1, top)) {
+                other = true;
+                break;
+            }
+        if (other) break;
+        checked = top;
+        const int32_t lo = base + i - (i & -i);
+        float v = fen[top];
+        for (int w = lo >> 5; w <= (top >> 5); w++) {
+            uint32_t mw = mark_word(mark, w, lo, top);
+            while (mw) {
+                const int bit = __ffs(mw) - 1;
+                mw &= mw - 1;
+                v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
+            }
+        }
+        fen[top] = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fen_update4(GridC g, const unsigned long long *__restrict__ list,
+                                                     const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const int32_t *__restrict__ capr, const float *__restrict__ lut,
                                                      float *__restrict__ fen) {
-    const int cnt = *owned_count;
+    const int cnt = *count;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const int32_t e = owned[t];
-        const int z = e / g.XY;
-        const int r = e - z * g.XY;
-        const int p = (z & 1) ? r % g.Y : r % g.X;
-        const int L = (z & 1) ? g.Y : g.X;
-        const int32_t base = e - p;
-        int32_t checked = e;  // no other marked cell in (e, checked]
-        for (int i = p + 1; i <= L; i += i & -i) {
-            const int32_t top = base + i - 1;
-            bool other = false;
-            for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
-                if (mark_word(mark, w, checked + 1, top)) {
-                    other = true;
-                    break;
-                }
-            if (other) break;
-            checked = top;
-            const int32_t lo = base + i - (i & -i);
-            float v = fen[top];
-            for (int w = lo >> 5; w <= (top >> 5); w++) {
-                uint32_t mw = mark_word(mark, w, lo, top);
-                while (mw) {
-                    const int bit = __ffs(mw) - 1;
-                    mw &= mw - 1;
-                    v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
-                }
-            }
-            fen[top] = v;
+        const unsigned long long it = list[t];
+        const int32_t w = (int32_t)(it >> 32);
+        uint32_t bits = (uint32_t)it;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            fen_owner_update(g, (w << 5) + b, mark, capr, lut, fen);
         }
     }
 }
 
-// demand += 1 for every marked cell; marks and owners cleared for the next batch
-__global__ void k_finalize3(const int32_t *__restrict__ owned, const int32_t *__restrict__ owned_count,
-                            uint32_t *__restrict__ mark, int32_t *__restrict__ owner, int32_t *__restrict__ capr) {
-    const int cnt = *owned_count;
+// demand += 1 for every marked cell; its marks cleared for the next batch
+__global__ void k_finalize4(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
+                            uint32_t *__restrict__ mark, int32_t *__restrict__ capr) {
+    const int cnt = *count;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const int32_t e = owned[t];
-        capr[e] -= 1;
-        owner[e] = -1;
-        atomicAnd(mark + (e >> 5), ~(1u << (e & 31)));
+        const unsigned long long it = list[t];
+        const int32_t w = (int32_t)(it >> 32);
+        const uint32_t bits0 = (uint32_t)it;
+        uint32_t bits = bits0;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            capr[(w << 5) + b] -= 1;
+        }
+        atomicAnd(mark + w, ~bits0);
     }
 }
 
