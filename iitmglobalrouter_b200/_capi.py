@@ -24,7 +24,7 @@ GR_ST_BAD_EDGE, GR_ST_BAD_PATTERN, GR_ST_MST_ROUNDS, GR_ST_BAD_PIN = 0x1, 0x2, 0
 GR_PLAN_GRAPH = 0x1
 GR_WRT_MERGE, GR_WRT_RSEG, GR_WRT_PPATCH = 0x1, 0x2, 0x4
 GR_MAX_PINS = 4096
-GR_PROF_KINDS = 8
+GR_PROF_KINDS = 10
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
 _P, _I, _I64, _U64, _D = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double

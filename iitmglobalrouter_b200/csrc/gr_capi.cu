@@ -8,6 +8,7 @@
 // pin offsets, so launches (and captured graphs) need no device readback.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -64,6 +65,8 @@ struct gr_ctx {
     int32_t n_nets = 0;
     std::vector<int64_t> h_pin_ofs;
     int32_t *d_pins = nullptr;
+    int32_t *d_pxy = nullptr, *d_cx = nullptr, *d_cy = nullptr;  // per-net coordinate indices and lists
+    std::vector<int32_t> h_nxy;                                    // per design net: (nx << 16) | ny
     // per-call batch descriptor (device) + pinned staging
     DevBuf desc, pcost, ppat, tab, dist;
     void *h_stage = nullptr;
@@ -85,6 +88,8 @@ struct gr_ctx {
     double prof_ms[GR_PROF_KINDS] = {};
     int64_t prof_n[GR_PROF_KINDS] = {};
     size_t pins_cap = 0;
+    void *h_coord_pinned = nullptr;  // pinned staging of the coordinate tables
+    size_t coord_cap = 0;
 };
 
 namespace {
@@ -101,6 +106,8 @@ constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
             return GR_ERR_CUDA;                                                                \
         }                                                                                      \
     } while (0)
+
+Coords coords(const gr_ctx *c) { return Coords{c->d_pxy, c->d_cx, c->d_cy}; }
 
 int grid_for(const gr_ctx *c, int64_t items, int per_sm = 8) {
     int64_t b = (items + kThreads - 1) / kThreads;
@@ -154,12 +161,14 @@ int ensure(DevBuf &b, size_t bytes, cudaStream_t s) {
 
 cudaStream_t pick(gr_ctx *c, void *stream) { return stream ? (cudaStream_t)stream : c->stream; }
 
-int64_t tab_entries(const gr_ctx *c, int n) {
-    return n <= kTableMaxPins ? (int64_t)c->g.Z * n * n : 0;
+// query-table entries of design net id (0: the net is costed by direct gathers)
+int64_t tab_entries(const gr_ctx *c, int32_t id) {
+    const int32_t nxy = c->h_nxy[id];
+    return (int64_t)c->g.Z * (nxy >> 16) * (nxy & 0xffff);
 }
 
 // bytes of a SoA descriptor of n nets
-size_t desc_bytes(int64_t n) { return (size_t)n * (2 * sizeof(int32_t) + 4 * sizeof(int64_t)) + 64; }
+size_t desc_bytes(int64_t n) { return (size_t)n * (3 * sizeof(int32_t) + 4 * sizeof(int64_t)) + 64; }
 
 // lays the SoA arrays of n nets out in a buffer (int64 arrays first)
 BatchView view_of(void *buf, int64_t total_n, int64_t first, int32_t n) {
@@ -171,8 +180,10 @@ BatchView view_of(void *buf, int64_t total_n, int64_t first, int32_t n) {
     int64_t *tab_ofs = node_ofs + total_n;
     int32_t *npin = (int32_t *)(tab_ofs + total_n);
     int32_t *order = npin + total_n;
+    int32_t *nxy = order + total_n;
     v.n = n;
     v.order = order + first;
+    v.nxy = nxy + first;
     v.npin = npin + first;
     v.pin_base = pin_base + first;
     v.pair_ofs = pair_ofs + first;
@@ -192,6 +203,7 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
     int64_t *tab_ofs = const_cast<int64_t *>(v.tab_ofs);
     int32_t *npin = const_cast<int32_t *>(v.npin);
     int32_t *order = const_cast<int32_t *>(v.order);
+    int32_t *nxy = const_cast<int32_t *>(v.nxy);
     int64_t P = 0, M = 0, T = 0;
     int32_t mp = 0, n2 = 0, nm = 0;
     for (int32_t i = 0; i < n; i++) {
@@ -206,7 +218,8 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
         tab_ofs[i] = T;
         P += (int64_t)k * (k - 1) / 2;
         M += k;
-        T += tab_entries(c, k);
+        T += tab_entries(c, id);
+        nxy[i] = c->h_nxy[id];
         if (k > mp) mp = k;
         n2 += k == 2;
         nm += k > 2 && k <= kMstWarpPins;
@@ -248,7 +261,7 @@ size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long 
 int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s) {
     if (v.n_tab > 0) {
         int pi = prof_begin(c, s);
-        k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab);
+        k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, coords(c), c->d_fen, tab);
         prof_end(c, s, pi, GR_K_QTABLE);
     }
     if (v.n_pairs > 0) {
@@ -256,13 +269,13 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
         const int grid = grid_for(c, v.n_pairs, 16);
 #define GR_LPAT_Z(ZV)                                                                                 \
     case ZV:                                                                                          \
-        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost, ppat);       \
+        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat); \
         break;
         switch (c->g.Z) {
             GR_LPAT_Z(3) GR_LPAT_Z(4) GR_LPAT_Z(5) GR_LPAT_Z(6) GR_LPAT_Z(7) GR_LPAT_Z(8) GR_LPAT_Z(9)
             GR_LPAT_Z(10) GR_LPAT_Z(11) GR_LPAT_Z(12) GR_LPAT_Z(13) GR_LPAT_Z(14) GR_LPAT_Z(15) GR_LPAT_Z(16)
             default:
-                k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, c->d_fen, tab, pcost, ppat);
+                k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat);
         }
 #undef GR_LPAT_Z
         prof_end(c, s, pi, GR_K_LPAT);
@@ -281,7 +294,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
     if (v.nm > 0) {
         int pi = prof_begin(c, s);
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
-        prof_end(c, s, pi, GR_K_MST);
+        prof_end(c, s, pi, GR_K_MST_WARP);
     }
     if (v.nl > 0) {
         // stage the pair costs of a net in shared memory when they fit
@@ -293,7 +306,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         int blocks = v.nl < c->sm_count * 4 ? v.nl : c->sm_count * 4;
         int pi = prof_begin(c, s);
         k_mst_large<<<blocks, 512, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status, stage);
-        prof_end(c, s, pi, GR_K_MST);
+        prof_end(c, s, pi, GR_K_MST_LARGE);
     }
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -308,7 +321,7 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
                                                            c->d_list, c->d_list_count, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update4<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_capr,
+    k_fen_update5<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_capr,
                                                         c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
@@ -472,6 +485,9 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_list);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
+    cudaFree(c->d_pxy);
+    cudaFree(c->d_cx);
+    cudaFree(c->d_cy);
     free_buf(c->desc);
     free_buf(c->pcost);
     free_buf(c->ppat);
@@ -479,6 +495,7 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->dist);
     free_buf(c->plan_desc);
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->h_coord_pinned) cudaFreeHost(c->h_coord_pinned);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     if (c->stage_done) cudaEventDestroy(c->stage_done);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -511,16 +528,68 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
     GR_CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
     if ((size_t)(total + 1) > c->pins_cap) {
-        if (c->d_pins) cudaFree(c->d_pins);
-        c->d_pins = nullptr;
+        for (int32_t **p : {&c->d_pins, &c->d_pxy, &c->d_cx, &c->d_cy}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
         c->pins_cap = 0;
-        if (cudaMalloc(&c->d_pins, sizeof(int32_t) * (total + 1)) != cudaSuccess) {
+        for (int32_t **p : {&c->d_pins, &c->d_pxy, &c->d_cx, &c->d_cy})
+            if (cudaMalloc(p, sizeof(int32_t) * (total + 1)) != cudaSuccess) {
+                cudaGetLastError();
+                return GR_ERR_NOMEM;
+            }
+        c->pins_cap = (size_t)(total + 1);
+    }
+    // per net: sorted distinct x and y coordinates and each pin's index into
+    // them (the query tables are laid out over these coordinates)
+    c->h_nxy.assign(n_nets, 0);
+    if ((size_t)(3 * total + 3) > c->coord_cap) {
+        if (c->h_coord_pinned) cudaFreeHost(c->h_coord_pinned);
+        c->h_coord_pinned = nullptr;
+        c->coord_cap = 0;
+        if (cudaMallocHost(&c->h_coord_pinned, sizeof(int32_t) * (3 * total + 3)) != cudaSuccess) {
             cudaGetLastError();
             return GR_ERR_NOMEM;
         }
-        c->pins_cap = (size_t)(total + 1);
+        c->coord_cap = (size_t)(3 * total + 3);
+    }
+    int32_t *hp = (int32_t *)c->h_coord_pinned, *hx = hp + total, *hy = hx + total;
+    const int X = c->g.X, Y = c->g.Y, XY = c->g.XY;
+#pragma omp parallel
+    {
+        std::vector<int32_t> xs, ys;
+#pragma omp for schedule(dynamic, 2048)
+        for (int32_t i = 0; i < n_nets; i++) {
+            const int64_t o = h_pin_ofs[i];
+            const int n = (int)(h_pin_ofs[i + 1] - o);
+            xs.resize(n);
+            ys.resize(n);
+            for (int a = 0; a < n; a++) {
+                const int32_t e = h_pins[o + a];
+                const int z = e / XY, r = e - z * XY;
+                xs[a] = (z & 1) ? r / Y : r % X;
+                ys[a] = (z & 1) ? r % Y : r / X;
+            }
+            std::vector<int32_t> ux(xs), uy(ys);
+            std::sort(ux.begin(), ux.end());
+            ux.erase(std::unique(ux.begin(), ux.end()), ux.end());
+            std::sort(uy.begin(), uy.end());
+            uy.erase(std::unique(uy.begin(), uy.end()), uy.end());
+            for (int a = 0; a < n; a++) {
+                const int xi = (int)(std::lower_bound(ux.begin(), ux.end(), xs[a]) - ux.begin());
+                const int yi = (int)(std::lower_bound(uy.begin(), uy.end(), ys[a]) - uy.begin());
+                hp[o + a] = (xi << 16) | yi;
+                hx[o + a] = a < (int)ux.size() ? ux[a] : 0;
+                hy[o + a] = a < (int)uy.size() ? uy[a] : 0;
+            }
+            const int64_t cells = (int64_t)ux.size() * uy.size();
+            c->h_nxy[i] = cells <= kTableMaxCells ? (int32_t)((ux.size() << 16) | uy.size()) : 0;
+        }
     }
     GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->d_pxy, hp, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->d_cx, hx, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->d_cy, hy, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
     c->h_pin_ofs.assign(h_pin_ofs, h_pin_ofs + n_nets + 1);
     c->n_nets = n_nets;
     c->plan.clear();
@@ -780,8 +849,9 @@ int gr_profile_read(gr_ctx *c, double *ms, int64_t *launches, int reset) {
 }
 
 const char *gr_kernel_name(int kind) {
-    static const char *names[GR_PROF_KINDS] = {"k_fen_init", "k_qtable", "k_lpat_batch", "k_mst", "k_mark",
-                                               "k_fen_update", "k_finalize", "k_lpat_pairs"};
+    static const char *names[GR_PROF_KINDS] = {"k_fen_init", "k_qtable", "k_lpat",   "k_mst_pin2",  "k_mark",
+                                               "k_fen_update", "k_finalize", "k_lpat_pairs", "k_mst_warp",
+                                               "k_mst_large"};
     return (kind >= 0 && kind < GR_PROF_KINDS) ? names[kind] : "";
 }
 

@@ -17,7 +17,7 @@ namespace gr {
 
 constexpr int kLutMin = -256;  // cost LUT covers remaining capacity [-256, 1024]
 constexpr int kLutMax = 1024;
-constexpr int kTableMaxPins = 1024;  // nets above this use direct Fenwick gathers
+constexpr int kTableMaxCells = 1 << 20;  // nx*ny above this: direct Fenwick gathers
 constexpr int kMstMaxRounds = 40;
 constexpr int kMstWarpPins = 32;   // nets up to this size: one warp each
 constexpr int kMaxLayers = 32;     // layer sets are 64-bit masks
@@ -186,45 +186,46 @@ struct DirectEv {
     __device__ bool at_dst(State s) const { return s.x == x2 && s.y == y2; }
 };
 
-// Prefix queries read from a per-net query table. For a net of n pins the
-// table holds, for every layer z and pin indices (a, b), the pair
+// Prefix queries read from a per-net query table. A net's pins have nx
+// distinct x and ny distinct y coordinates; for every layer z and indices
+// (a, b) into those sorted lists the table holds the pair
 //   even z: (Q(z, row y_b, x_a), Q(z, row y_b, x_a - 1))
 //   odd  z: (Q(z, col x_a, y_b), Q(z, col x_a, y_b - 1))
-// at tab[(z*n + a)*n + b]. A pattern of pair (j -> k) only visits the four
+// at tab[(z*nx + a)*ny + b]. A pattern of pair (j -> k) only visits the four
 // points {x_j, x_k} x {y_j, y_k}, so every query it makes is in the table.
 struct TableEv {
     struct State {
-        int a, b;  // pin index giving x, pin index giving y
+        bool ak, bk;  // x taken from pin k (else j), y taken from pin k (else j)
     };
     const float2 *tab;
-    int n, j, k;
+    int nx, ny, xij, yij, xik, yik;  // coordinate indices of pins j and k
     int z1, z2, xj, yj, xk, yk;
     bool bth;
-    __device__ State start() const { return State{j, j}; }
-    __device__ float2 t(int z, int a, int b) const { return tab[((int64_t)z * n + a) * n + b]; }
-    __device__ int xof(int a) const { return a == j ? xj : xk; }
-    __device__ int yof(int b) const { return b == j ? yj : yk; }
+    __device__ State start() const { return State{false, false}; }
+    __device__ float2 t(int z, bool ak, bool bk) const {
+        return tab[((int64_t)z * nx + (ak ? xik : xij)) * ny + (bk ? yik : yij)];
+    }
     __device__ void via(int za, int zb, State s, float &c) const {
         int zmin = za < zb ? za : zb, zmax = za < zb ? zb : za;
         for (int i = zmin; i < zmax; i++) {
-            float2 q = t(i, s.a, s.b);
+            float2 q = t(i, s.ak, s.bk);
             c += q.x - q.y;
         }
     }
     __device__ void wire(int z, State &s, float &c) const {
         if (z & 1) {
-            int yb = yof(s.b);
-            if (yb < yk) c += t(z, s.a, k).x - t(z, s.a, s.b).y;
-            else if (yb > yk) c += t(z, s.a, s.b).x - t(z, s.a, k).y;
-            s.b = k;
+            int yb = s.bk ? yk : yj;
+            if (yb < yk) c += t(z, s.ak, true).x - t(z, s.ak, s.bk).y;
+            else if (yb > yk) c += t(z, s.ak, s.bk).x - t(z, s.ak, true).y;
+            s.bk = true;
         } else {
-            int xa = xof(s.a);
-            if (xa < xk) c += t(z, k, s.b).x - t(z, s.a, s.b).y;
-            else if (xa > xk) c += t(z, s.a, s.b).x - t(z, k, s.b).y;
-            s.a = k;
+            int xa = s.ak ? xk : xj;
+            if (xa < xk) c += t(z, true, s.bk).x - t(z, s.ak, s.bk).y;
+            else if (xa > xk) c += t(z, s.ak, s.bk).x - t(z, true, s.bk).y;
+            s.ak = true;
         }
     }
-    __device__ bool at_dst(State s) const { return xof(s.a) == xk && yof(s.b) == yk; }
+    __device__ bool at_dst(State s) const { return (s.ak ? xk : xj) == xk && (s.bk ? yk : yj) == yk; }
 };
 
 }  // namespace gr

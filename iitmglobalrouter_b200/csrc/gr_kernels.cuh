@@ -7,7 +7,7 @@
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
 //   k_mark4        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update4  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_fen_update5  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
 //   k_finalize4    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
@@ -24,9 +24,19 @@ struct BatchView {
     const int64_t *node_ofs;  // [n] prefix of n (MST slots)
     const int64_t *tab_ofs;   // [n] prefix of query-table entries
     const int32_t *order;     // [n] net indices: 2-pin nets, then 3..32 pins, then larger
+    const int32_t *nxy;       // [n] (distinct x count << 16) | distinct y count; 0: no table
     int64_t n_pairs, n_nodes, n_tab;
     int32_t max_pins;
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
+};
+
+// Per design pin (indexed like the pin array): the pin's index into its net's
+// sorted distinct x and y lists, packed (xi << 16) | yi; and the lists
+// themselves, stored from the net's first pin slot on.
+struct Coords {
+    const int32_t *pxy;
+    const int32_t *cx;
+    const int32_t *cy;
 };
 
 __device__ __forceinline__ float lut_cost(const float *__restrict__ lut, int c) {
@@ -60,23 +70,22 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
 }
 
 // ---------------------------------------------------------------- query table
-__global__ void k_qtable(GridC g, BatchView bv, const int32_t *__restrict__ pins, const float *__restrict__ fen,
-                         float2 *__restrict__ tab) {
+// Entry (z, a, b) of a net's table: the two prefix queries at (x_a, y_b) on
+// layer z along the layer's direction (x on even layers, y on odd ones).
+__global__ void k_qtable(GridC g, BatchView bv, Coords cd, const float *__restrict__ fen, float2 *__restrict__ tab) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < bv.n_tab;
          t += (int64_t)gridDim.x * blockDim.x) {
-        int net = ofs_search(bv.tab_ofs, bv.n, t);
-        int64_t local = t - bv.tab_ofs[net];
-        int n = bv.npin[net];
-        int64_t nn = (int64_t)n * n;
-        int z = (int)(local / nn);
-        int r = (int)(local - z * nn);
-        int a = r / n, b = r - a * n;
-        const int32_t *np = pins + bv.pin_base[net];
-        int za, xa, ya, zb, xb, yb;
-        dec(g, __ldg(np + a), za, xa, ya);
-        dec(g, __ldg(np + b), zb, xb, yb);
-        int32_t base = track_base(g, z, xa, yb);
-        int pos = (z & 1) ? yb : xa;
+        const int net = ofs_search(bv.tab_ofs, bv.n, t);
+        const int64_t local = t - bv.tab_ofs[net];
+        const int nxy = bv.nxy[net], nx = nxy >> 16, ny = nxy & 0xffff;
+        const int per = nx * ny;
+        const int z = (int)(local / per);
+        const int r = (int)(local - (int64_t)z * per);
+        const int a = r / ny, b = r - a * ny;
+        const int64_t pb = bv.pin_base[net];
+        const int x = __ldg(cd.cx + pb + a), y = __ldg(cd.cy + pb + b);
+        const int32_t base = track_base(g, z, x, y);
+        const int pos = (z & 1) ? y : x;
         float2 q;
         q.x = fen_query(fen, base, pos);
         q.y = fen_query(fen, base, pos - 1);
@@ -86,12 +95,12 @@ __global__ void k_qtable(GridC g, BatchView bv, const int32_t *__restrict__ pins
 
 // ---------------------------------------------------------------- L-pattern
 __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const int32_t *__restrict__ pins,
-                                                    const float *__restrict__ fen, const float2 *__restrict__ tab,
+                                                    Coords cd, const float *__restrict__ fen,
+                                                    const float2 *__restrict__ tab,
                                                     float *__restrict__ cost, int16_t *__restrict__ pat) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
          p += (int64_t)gridDim.x * blockDim.x) {
         int net = ofs_search(bv.pair_ofs, bv.n, p);
-        int n = bv.npin[net];
         int j, k;
         pair_decode(p - bv.pair_ofs[net], j, k);
         const int32_t *np = pins + bv.pin_base[net];
@@ -100,12 +109,17 @@ __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const
         dec(g, __ldg(np + k), z2, x2, y2);
         float c;
         int cp;
-        if (n <= kTableMaxPins) {
+        const int nxy = bv.nxy[net];
+        if (nxy) {
+            const int pj = __ldg(cd.pxy + bv.pin_base[net] + j), pk = __ldg(cd.pxy + bv.pin_base[net] + k);
             TableEv ev;
             ev.tab = tab + bv.tab_ofs[net];
-            ev.n = n;
-            ev.j = j;
-            ev.k = k;
+            ev.nx = nxy >> 16;
+            ev.ny = nxy & 0xffff;
+            ev.xij = pj >> 16;
+            ev.yij = pj & 0xffff;
+            ev.xik = pk >> 16;
+            ev.yik = pk & 0xffff;
             ev.z1 = z1;
             ev.z2 = z2;
             ev.xj = x1;
@@ -329,12 +343,13 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
 // (bit_util.hpp:36-38). With Z a compile-time constant the 6Z values stay
 // in registers and every pattern is summed in path order from them.
 template <int ZC>
-__device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int n, int j, int k, int z1, int z2, int xj,
-                                          int yj, int xk, int yk, float &out_c, int &out_p) {
+__device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
+                                          int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p) {
     constexpr int Z2 = (ZC + 1) / 2;
     float Pj[ZC], Pk[ZC], Pc1[ZC], Pc2[ZC], W1[ZC], W2[ZC];
-    const int64_t nn = (int64_t)n * n;
-    const int ojj = j * n + j, okk = k * n + k, okj = k * n + j, ojk = j * n + k;
+    const int64_t nn = (int64_t)nx * ny;
+    const int xij = pj >> 16, yij = pj & 0xffff, xik = pk >> 16, yik = pk & 0xffff;
+    const int ojj = xij * ny + yij, okk = xik * ny + yik, okj = xik * ny + yij, ojk = xij * ny + yik;
     const bool xlt = xj < xk, ylt = yj < yk;
     const bool mx = xj != xk, my = yj != yk;
 #pragma unroll
@@ -411,13 +426,12 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int n, i
 }
 
 template <int ZC>
-__global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+__global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
                                                 float *__restrict__ cost, int16_t *__restrict__ pat) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int net = ofs_search(bv.pair_ofs, bv.n, p);
-        const int n = bv.npin[net];
         int j, k;
         pair_decode(p - bv.pair_ofs[net], j, k);
         const int32_t *np = pins + bv.pin_base[net];
@@ -426,8 +440,11 @@ __global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int
         dec(g, __ldg(np + k), z2, x2, y2);
         float c;
         int cp;
-        if (n <= kTableMaxPins) {
-            lpat_regs<ZC>(tab + bv.tab_ofs[net], n, j, k, z1, z2, x1, y1, x2, y2, c, cp);
+        const int nxy = bv.nxy[net];
+        if (nxy) {
+            const int64_t pb = bv.pin_base[net];
+            lpat_regs<ZC>(tab + bv.tab_ofs[net], nxy >> 16, nxy & 0xffff, __ldg(cd.pxy + pb + j),
+                          __ldg(cd.pxy + pb + k), z1, z2, x1, y1, x2, y2, c, cp);
         } else {
             DirectEv ev{fen, g, z1, x1, y1, z2, x2, y2, (x1 != x2 && y1 != y2)};
             lpat_argmin(ev, g, c, cp);
@@ -711,21 +728,47 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
     }
 }
 
-__global__ void __launch_bounds__(256) k_fen_update4(GridC g, const unsigned long long *__restrict__ list,
+// Each warp takes 32 list entries, prefix-sums their bit counts and hands the
+// cells out one per lane (the r-th set bit of an entry via __fns).
+__global__ void __launch_bounds__(256) k_fen_update5(GridC g, const unsigned long long *__restrict__ list,
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const int32_t *__restrict__ capr, const float *__restrict__ lut,
                                                      float *__restrict__ fen) {
+    __shared__ int sx[8][32];
+    __shared__ unsigned long long se[8][32];
     const int cnt = *count;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const unsigned long long it = list[t];
-        const int32_t w = (int32_t)(it >> 32);
-        uint32_t bits = (uint32_t)it;
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            fen_owner_update(g, (w << 5) + b, mark, capr, lut, fen);
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int e0 = (blockIdx.x * (blockDim.x >> 5) + wib) * 32; e0 < cnt; e0 += warps * 32) {
+        const int ei = e0 + lane;
+        const unsigned long long it = ei < cnt ? list[ei] : 0ull;
+        const int c = __popc((uint32_t)it);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
         }
+        const int total = __shfl_sync(FULL, incl, 31);
+        sx[wib][lane] = incl - c;
+        se[wib][lane] = it;
+        __syncwarp();
+        for (int t = lane; t < total; t += 32) {
+            int lo = 0, hi = 31;  // last entry whose exclusive prefix is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sx[wib][mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            const unsigned long long en = se[wib][lo];
+            uint32_t m = (uint32_t)en;
+            for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
+            const int b = __ffs(m) - 1;
+            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + b, mark, capr, lut, fen);
+        }
+        __syncwarp();
     }
 }
 

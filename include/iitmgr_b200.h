@@ -155,7 +155,9 @@ int64_t gr_launch_count(gr_ctx *ctx);
 #define GR_K_FEN_UPDATE 5
 #define GR_K_FINALIZE 6
 #define GR_K_LPAT_PAIRS 7
-#define GR_PROF_KINDS 8
+#define GR_K_MST_WARP 8
+#define GR_K_MST_LARGE 9
+#define GR_PROF_KINDS 10
 int gr_profile_enable(gr_ctx *ctx, int on);
 int gr_profile_read(gr_ctx *ctx, double *ms, int64_t *launches, int reset);
 const char *gr_kernel_name(int kind);
