@@ -37,6 +37,7 @@ struct BatchInfo {  // one batch of a plan
     int64_t n_pairs, n_nodes, n_tab, slot0;
     int32_t max_pins;
     int32_t n2, nm, nl;  // nets of 2 pins, 3..32 pins, more
+    int32_t nmid;        // of the nl larger nets, those up to kMstMidPins pins (listed first)
 };
 
 struct GraphCache {
@@ -59,6 +60,7 @@ struct gr_ctx {
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
     unsigned long long *d_list = nullptr;  // (word, newly set bits) of a batch's marked cells
+    uint32_t *d_sum = nullptr;             // one bit per mark word holding any mark
     int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
     // design
@@ -96,6 +98,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
+constexpr int kMstMidPins = 128;         // k_mst_large on 128 threads up to this size
 
 #define GR_CK(call)                                                                            \
     do {                                                                                       \
@@ -224,15 +227,19 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
         n2 += k == 2;
         nm += k > 2 && k <= kMstWarpPins;
     }
-    // nets by size class (k_mst_pin2 / k_mst_warp / k_mst_large), batch order kept
-    int32_t o2 = 0, om = n2, ol = n2 + nm;
+    // nets by size class (k_mst_pin2 / k_mst_warp / k_mst_large on 128 or 512
+    // threads), batch order kept within a class
+    int32_t nmid = 0;
+    for (int32_t i = 0; i < n; i++) nmid += npin[i] > kMstWarpPins && npin[i] <= kMstMidPins;
+    int32_t o2 = 0, om = n2, oi = n2 + nm, ol = n2 + nm + nmid;
     for (int32_t i = 0; i < n; i++) {
         const int32_t k = npin[i];
-        order[k == 2 ? o2++ : (k <= kMstWarpPins ? om++ : ol++)] = i;
+        order[k == 2 ? o2++ : (k <= kMstWarpPins ? om++ : (k <= kMstMidPins ? oi++ : ol++))] = i;
     }
     bi.n2 = n2;
     bi.nm = nm;
     bi.nl = n - n2 - nm;
+    bi.nmid = nmid;
     bi.first = first;
     bi.n = n;
     bi.n_pairs = P;
@@ -251,6 +258,7 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
     v.n2 = bi.n2;
     v.nm = bi.nm;
     v.nl = bi.nl;
+    v.nmid = bi.nmid;
     return v;
 }
 
@@ -296,16 +304,24 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s, pi, GR_K_MST_WARP);
     }
-    if (v.nl > 0) {
-        // stage the pair costs of a net in shared memory when they fit
-        const int64_t maxp = (int64_t)v.max_pins * (v.max_pins - 1) / 2;
-        const size_t base = mst_smem(v.max_pins);
+    // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above; the
+    // pair costs of a net are staged in shared memory when they fit
+    const int nmid = v.nmid, nbig = v.nl - v.nmid;
+    for (int part = 0; part < 2; part++) {
+        const int cnt = part ? nbig : nmid;
+        if (cnt <= 0) continue;
+        const int maxn = part ? v.max_pins : (v.max_pins < kMstMidPins ? v.max_pins : kMstMidPins);
+        const int64_t maxp = (int64_t)maxn * (maxn - 1) / 2;
+        const size_t base = mst_smem(maxn);
         const int64_t room = ((int64_t)kMstSmemMax - (int64_t)base) / 4;
         const int64_t stage = maxp < room ? maxp : room;  // nets with at most `stage` pairs are staged
         const size_t sm = base + (size_t)stage * 4;
-        int blocks = v.nl < c->sm_count * 4 ? v.nl : c->sm_count * 4;
+        const int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
+        BatchView vv = v;
+        vv.max_pins = maxn;
         int pi = prof_begin(c, s);
-        k_mst_large<<<blocks, 512, sm, s>>>(c->g, v, pcost, mst, dist, c->d_status, stage);
+        k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, stage,
+                                                          v.n2 + v.nm + (part ? nmid : 0), cnt);
         prof_end(c, s, pi, GR_K_MST_LARGE);
     }
     GR_CK(cudaGetLastError());
@@ -317,15 +333,15 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     if (v.n_nodes <= 0) return GR_OK;
     GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
-    k_mark4<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                           c->d_list, c->d_list_count, c->d_status);
+    k_mark5<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
+                                                           c->d_sum, c->d_list, c->d_list_count, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update5<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_capr,
-                                                        c->d_lut, c->d_fen);
+    k_fen_update6<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
+                                                        c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
-    k_finalize4<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_capr);
+    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum, c->d_capr);
     prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -448,6 +464,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
         cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list, sizeof(unsigned long long) * (size_t)csize) ||
         cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -459,7 +476,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
         cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_list_count, 0, 16))
+        cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_sum, 0, (words / 32 + 2) * 4))
         return fail(GR_ERR_CUDA);
     c->mst_smem_max = kMstSmemMax;
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
@@ -483,6 +500,7 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
     cudaFree(c->d_list);
+    cudaFree(c->d_sum);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
     cudaFree(c->d_pxy);
@@ -508,6 +526,7 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
+    GR_CK(cudaMemsetAsync(c->d_sum, 0, sizeof(uint32_t) * (size_t)(c->csize / 1024 + 2), s));
     int pi = prof_begin(c, s);
     k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_INIT);

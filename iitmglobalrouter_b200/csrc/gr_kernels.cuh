@@ -6,9 +6,9 @@
 //   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
-//   k_mark4        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update5  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize4    demand += 1 per marked cell, marks cleared
+//   k_mark5        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_fen_update6  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_finalize5    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
 
@@ -28,6 +28,7 @@ struct BatchView {
     int64_t n_pairs, n_nodes, n_tab;
     int32_t max_pins;
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
+    int32_t nmid;             // of the nl larger nets, the first nmid have at most 128 pins
 };
 
 // Per design pin (indexed like the pin array): the pin's index into its net's
@@ -209,7 +210,7 @@ __device__ __forceinline__ int64_t pair_id(int a, int b) {
 
 __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                   uint32_t *status, int64_t stage_pairs) {
+                                                   uint32_t *status, int64_t stage_pairs, int first, int count) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_nrec, s_changed;
@@ -222,8 +223,8 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
     int *flag = mx + maxn;
     const int B = blockDim.x, tid = threadIdx.x;
     float *wsm = (float *)(flag + maxn);  // pair costs, when the net's fit
-    for (int t = blockIdx.x; t < bv.nl; t += gridDim.x) {
-        const int net = bv.order[bv.n2 + bv.nm + t];
+    for (int t = blockIdx.x; t < count; t += gridDim.x) {
+        const int net = bv.order[first + t];
         const int n = bv.npin[net];
         const int64_t P = (int64_t)n * (n - 1) / 2;
         const float *w = cost + bv.pair_ofs[net];
@@ -630,64 +631,108 @@ __device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, cons
 }
 
 // Marks with one atomicOr per bitmap word. The bits a slot sets first are
-// the cells it owns for this batch; each (word, newly set bits) pair is
-// appended to the batch's list with one warp-aggregated atomic.
-__device__ __forceinline__ void list_append(unsigned long long *list, int32_t *count, int32_t w, uint32_t bits) {
-    const unsigned active = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(active) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(count, __popc(active));
-    base = __shfl_sync(active, base, leader);
-    list[base + __popc(active & ((1u << lane) - 1))] = ((unsigned long long)(uint32_t)w << 32) | bits;
-}
+// the cells it owns for this batch; the slot lists them as (word, newly set
+// bits) entries. A summary bitmap holds one bit per mark word that has any
+// mark, so range scans skip empty 1024-cell blocks.
+constexpr int kEntBuf = 24;
 
 struct MarkVis {
     uint32_t *mark;
+    uint32_t *sum;
     unsigned long long *list;
     int32_t *count;
-    __device__ __forceinline__ void span(int32_t e0, int n) {
-        const int32_t e1 = e0 + n - 1;
+    unsigned long long ent[kEntBuf];
+    int n = 0;
+    __device__ __forceinline__ void add(int32_t w, uint32_t bits) {
+        const unsigned long long v = ((unsigned long long)(uint32_t)w << 32) | bits;
+        if (n < kEntBuf) ent[n++] = v;
+        else list[atomicAdd(count, 1)] = v;  // long paths: the rare overflow goes out one by one
+    }
+    __device__ __forceinline__ void word(int w, uint32_t m) {
+        const uint32_t old = atomicOr(mark + w, m);
+        const uint32_t nb = m & ~old;
+        if (nb) {
+            if (!old) atomicOr(sum + (w >> 5), 1u << (w & 31));
+            add(w, nb);
+        }
+    }
+    __device__ __forceinline__ void span(int32_t e0, int cnt) {
+        const int32_t e1 = e0 + cnt - 1;
         for (int w = e0 >> 5; w <= (e1 >> 5); w++) {
             uint32_t m = 0xffffffffu;
             if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
             if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
-            const uint32_t nb = m & ~atomicOr(mark + w, m);
-            if (nb) list_append(list, count, w, nb);
+            word(w, m);
         }
     }
-    __device__ __forceinline__ void cell(int32_t e) {
-        const uint32_t bit = 1u << (e & 31);
-        if (!(atomicOr(mark + (e >> 5), bit) & bit)) list_append(list, count, e >> 5, bit);
-    }
+    __device__ __forceinline__ void cell(int32_t e) { word(e >> 5, 1u << (e & 31)); }
 };
 
-// One thread per MST slot: mark the GCELLs of its edge.
-__global__ void __launch_bounds__(256) k_mark4(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+// One thread per MST slot: mark the GCELLs of its edge, then append its
+// entries contiguously (one warp scan and one atomic per warp), so the cells
+// of a path stay together in the list.
+__global__ void __launch_bounds__(256) k_mark5(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                               int32_t *__restrict__ mst_pat, uint32_t *mark,
+                                               int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *sum,
                                                unsigned long long *__restrict__ list, int32_t *count,
                                                uint32_t *status) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
-         s += (int64_t)gridDim.x * blockDim.x) {
-        EdgeRef r;
-        const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
-        if (ok <= 0) {
-            if (mst_pat) mst_pat[s] = -1;
-            if (ok < 0) atomicOr(status, 0x1u);
-            continue;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < bv.n_nodes; s0 += stride) {
+        const int64_t s = s0 + lane;
+        MarkVis vis{mark, sum, list, count};
+        if (s < bv.n_nodes) {
+            EdgeRef r;
+            const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
+            if (ok <= 0) {
+                if (mst_pat) mst_pat[s] = -1;
+                if (ok < 0) atomicOr(status, 0x1u);
+            } else {
+                if (mst_pat) mst_pat[s] = r.cpat;
+                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
+            }
         }
-        if (mst_pat) mst_pat[s] = r.cpat;
-        MarkVis vis{mark, list, count};
-        if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
+        __syncwarp();
+        int incl = vis.n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        int base = 0;
+        if (lane == 31 && total) base = atomicAdd(count, total);
+        base = __shfl_sync(FULL, base, 31) + incl - vis.n;
+        for (int t = 0; t < vis.n; t++) list[base + t] = vis.ent[t];
     }
 }
 
-__device__ __forceinline__ uint32_t mark_word(const uint32_t *__restrict__ mark, int w, int32_t lo, int32_t hi) {
-    uint32_t m = __ldg(mark + w);
-    if (w == (lo >> 5)) m &= 0xffffffffu << (lo & 31);
-    if (w == (hi >> 5)) m &= 0xffffffffu >> (31 - (hi & 31));
-    return m;
+// Visits the marked cells of [lo, hi] in ascending order; f(cell) returns
+// false to stop. Reads one summary word per 1024 cells and only the non-empty
+// mark words.
+template <class F>
+__device__ __forceinline__ void scan_marks(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
+                                           int32_t lo, int32_t hi, F &&f) {
+    if (lo > hi) return;
+    const int wlo = lo >> 5, whi = hi >> 5;
+    for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
+        uint32_t sm = __ldg(sum + sw);
+        if (sw == (wlo >> 5)) sm &= 0xffffffffu << (wlo & 31);
+        if (sw == (whi >> 5)) sm &= 0xffffffffu >> (31 - (whi & 31));
+        while (sm) {
+            const int w = (sw << 5) + __ffs(sm) - 1;
+            sm &= sm - 1;
+            uint32_t m = __ldg(mark + w);
+            if (w == wlo) m &= 0xffffffffu << (lo & 31);
+            if (w == whi) m &= 0xffffffffu >> (31 - (hi & 31));
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                if (!f((w << 5) + b)) return;
+            }
+        }
+    }
 }
 
 // For a marked cell at track position p: walk its update path
@@ -696,8 +741,8 @@ __device__ __forceinline__ uint32_t mark_word(const uint32_t *__restrict__ mark,
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
 __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
-                                                 const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                 float *__restrict__ fen) {
+                                                 const uint32_t *__restrict__ sum, const int32_t *__restrict__ capr,
+                                                 const float *__restrict__ lut, float *__restrict__ fen) {
     const int z = e / g.XY;
     const int r = e - z * g.XY;
     const int p = (z & 1) ? r % g.Y : r % g.X;
@@ -707,32 +752,27 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
     for (int i = p + 1; i <= L; i += i & -i) {
         const int32_t top = base + i - 1;
         bool other = false;
-        for (int w = (checked + 1) >> 5; w <= (top >> 5) && checked < top; w++)
-            if (mark_word(mark, w, checked + 1, top)) {
-                other = true;
-                break;
-            }
+        scan_marks(mark, sum, checked + 1, top, [&](int32_t) {
+            other = true;
+            return false;
+        });
         if (other) break;
         checked = top;
-        const int32_t lo = base + i - (i & -i);
         float v = fen[top];
-        for (int w = lo >> 5; w <= (top >> 5); w++) {
-            uint32_t mw = mark_word(mark, w, lo, top);
-            while (mw) {
-                const int bit = __ffs(mw) - 1;
-                mw &= mw - 1;
-                v += lut_inc(lut, __ldg(capr + (w << 5) + bit));
-            }
-        }
+        scan_marks(mark, sum, base + i - (i & -i), top, [&](int32_t q) {
+            v += lut_inc(lut, __ldg(capr + q));
+            return true;
+        });
         fen[top] = v;
     }
 }
 
 // Each warp takes 32 list entries, prefix-sums their bit counts and hands the
-// cells out one per lane (the r-th set bit of an entry via __fns).
-__global__ void __launch_bounds__(256) k_fen_update5(GridC g, const unsigned long long *__restrict__ list,
+// cells out one per lane.
+__global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned long long *__restrict__ list,
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
+                                                     const uint32_t *__restrict__ sum,
                                                      const int32_t *__restrict__ capr, const float *__restrict__ lut,
                                                      float *__restrict__ fen) {
     __shared__ int sx[8][32];
@@ -765,16 +805,16 @@ __global__ void __launch_bounds__(256) k_fen_update5(GridC g, const unsigned lon
             const unsigned long long en = se[wib][lo];
             uint32_t m = (uint32_t)en;
             for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            const int b = __ffs(m) - 1;
-            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + b, mark, capr, lut, fen);
+            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, lut, fen);
         }
         __syncwarp();
     }
 }
 
-// demand += 1 for every marked cell; its marks cleared for the next batch
-__global__ void k_finalize4(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
-                            uint32_t *__restrict__ mark, int32_t *__restrict__ capr) {
+// demand += 1 for every marked cell; marks (and emptied summary bits)
+// cleared for the next batch
+__global__ void k_finalize5(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
+                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum, int32_t *__restrict__ capr) {
     const int cnt = *count;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const unsigned long long it = list[t];
@@ -786,7 +826,8 @@ __global__ void k_finalize4(const unsigned long long *__restrict__ list, const i
             bits &= bits - 1;
             capr[(w << 5) + b] -= 1;
         }
-        atomicAnd(mark + w, ~bits0);
+        const uint32_t old = atomicAnd(mark + w, ~bits0);
+        if ((old & ~bits0) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
     }
 }
 
