@@ -61,6 +61,8 @@ struct gr_ctx {
     uint32_t *d_mark = nullptr, *d_status = nullptr;
     unsigned long long *d_list = nullptr;  // (word, newly set bits) of a batch's marked cells
     uint32_t *d_sum = nullptr;             // one bit per mark word holding any mark
+    float *d_dlt = nullptr;                // cost increment of each cell marked in the batch
+    DevBuf mat;                            // per-CTA pair-cost matrices of the largest nets
     int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
     // design
@@ -262,7 +264,10 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
     return v;
 }
 
-size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long long) + 5 * sizeof(int)); }
+// k_mst_large shared memory: per pin a 64-bit key, five ints and a float
+size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long long) + 6 * sizeof(int)); }
+// whether a net of n pins keeps its n x n cost matrix in shared memory
+bool mst_mat_in_smem(int n) { return mst_smem(n) + (size_t)n * n * sizeof(float) <= (size_t)kMstSmemMax; }
 
 // ------------------------------------------------------------------ stages
 
@@ -304,24 +309,29 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s, pi, GR_K_MST_WARP);
     }
-    // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above; the
-    // pair costs of a net are staged in shared memory when they fit
+    // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above; a
+    // net's full cost matrix sits in shared memory when it fits, else in a
+    // per-CTA global scratch (sized by ensure_mst_scratch)
     const int nmid = v.nmid, nbig = v.nl - v.nmid;
     for (int part = 0; part < 2; part++) {
         const int cnt = part ? nbig : nmid;
         if (cnt <= 0) continue;
         const int maxn = part ? v.max_pins : (v.max_pins < kMstMidPins ? v.max_pins : kMstMidPins);
-        const int64_t maxp = (int64_t)maxn * (maxn - 1) / 2;
-        const size_t base = mst_smem(maxn);
-        const int64_t room = ((int64_t)kMstSmemMax - (int64_t)base) / 4;
-        const int64_t stage = maxp < room ? maxp : room;  // nets with at most `stage` pairs are staged
-        const size_t sm = base + (size_t)stage * 4;
-        const int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
+        const bool in_smem = mst_mat_in_smem(maxn);
+        const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
+        int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
+        float *gmat = nullptr;
+        if (!in_smem) {
+            blocks = cnt < c->sm_count ? cnt : c->sm_count;
+            if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
+            gmat = (float *)c->mat.p;
+        }
         BatchView vv = v;
         vv.max_pins = maxn;
         int pi = prof_begin(c, s);
-        k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, stage,
-                                                          v.n2 + v.nm + (part ? nmid : 0), cnt);
+        k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
+                                                          (int64_t)maxn * maxn, v.n2 + v.nm + (part ? nmid : 0),
+                                                          cnt);
         prof_end(c, s, pi, GR_K_MST_LARGE);
     }
     GR_CK(cudaGetLastError());
@@ -334,14 +344,15 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
     k_mark5<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                           c->d_sum, c->d_list, c->d_list_count, c->d_status);
+                                                           c->d_sum, c->d_list, c->d_list_count, c->d_capr,
+                                                           c->d_dlt, c->d_lut, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
     k_fen_update6<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
-                                                        c->d_capr, c->d_lut, c->d_fen);
+                                                        c->d_dlt, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
-    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum, c->d_capr);
+    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum);
     prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -350,6 +361,13 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
 int check_mst_smem(gr_ctx *c, int max_pins) {
     if (max_pins > GR_MAX_PINS) return GR_ERR_NET_TOO_LARGE;
     return GR_OK;
+}
+
+// global pair-cost matrices for k_mst_large when a batch's largest net
+// does not fit in shared memory (one matrix per CTA, at most one CTA per SM)
+int ensure_mst_scratch(gr_ctx *c, int max_pins, cudaStream_t s) {
+    if (max_pins <= kMstMidPins || mst_mat_in_smem(max_pins)) return GR_OK;
+    return ensure(c->mat, (size_t)c->sm_count * max_pins * max_pins * sizeof(float), s);
 }
 
 // scratch for one batch of the given sizes
@@ -385,6 +403,7 @@ int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchV
     int rc = fill_desc(c, ids, n, c->h_stage, n, 0, bi);
     if (rc) return rc;
     if ((rc = check_mst_smem(c, bi.max_pins))) return rc;
+    if ((rc = ensure_mst_scratch(c, bi.max_pins, s))) return rc;
     if ((rc = ensure(c->desc, bytes, s))) return rc;
     GR_CK(cudaMemcpyAsync(c->desc.p, c->h_stage, bytes, cudaMemcpyHostToDevice, s));
     GR_CK(cudaEventRecord(c->stage_done, s));
@@ -464,7 +483,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
         cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list, sizeof(unsigned long long) * (size_t)csize) ||
         cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
-        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) ||
+        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) || cudaMalloc(&c->d_dlt, cell4 + 128) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -501,6 +520,8 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_status);
     cudaFree(c->d_list);
     cudaFree(c->d_sum);
+    cudaFree(c->d_dlt);
+    free_buf(c->mat);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
     cudaFree(c->d_pxy);
@@ -699,6 +720,9 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
         if (plan[b].n > mn) mn = plan[b].n;
     }
     int rc;
+    int32_t plan_max_pins = 0;
+    for (const BatchInfo &bi : plan) plan_max_pins = bi.max_pins > plan_max_pins ? bi.max_pins : plan_max_pins;
+    if ((rc = ensure_mst_scratch(c, plan_max_pins, c->stream))) return rc;
     if ((rc = ensure(c->plan_desc, bytes, c->stream))) return rc;
     GR_CK(cudaMemcpyAsync(c->plan_desc.p, host, bytes, cudaMemcpyHostToDevice, c->stream));
     GR_CK(cudaEventRecord(c->stage_done, c->stream));

@@ -65,6 +65,13 @@ __device__ __forceinline__ unsigned long long cost_key(float w, uint32_t e) {
     return ((unsigned long long)u << 32) | (unsigned long long)e;
 }
 
+// the cost whose key this is (exact inverse of cost_key's order transform)
+__device__ __forceinline__ float key_cost(unsigned long long key) {
+    uint32_t u = (uint32_t)(key >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    return __uint_as_float(u);
+}
+
 // decode a local pair id e = j(j-1)/2 + k (k < j), gmst_util.hpp:192-194
 __device__ __forceinline__ void pair_decode(long long e, int &j, int &k) {
     long long jj = (long long)((1.0 + sqrt(1.0 + 8.0 * (double)e)) * 0.5);

@@ -6,9 +6,9 @@
 //   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
-//   k_mark5        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_mark5        GCELLs of every MST edge, batch-deduped, demand += 1 (mst_bit_commit.hpp:81-235)
 //   k_fen_update6  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize5    demand += 1 per marked cell, marks cleared
+//   k_finalize5    marks cleared for the next batch
 #pragma once
 #include "gr_device.cuh"
 
@@ -208,12 +208,17 @@ __device__ __forceinline__ int64_t pair_id(int a, int b) {
     return a > b ? (int64_t)a * (a - 1) / 2 + b : (int64_t)b * (b - 1) / 2 + a;
 }
 
+// The net's pair costs are first spread into a full symmetric n x n matrix
+// (shared memory when it fits, else this CTA's global scratch) so that each
+// pin's crossing scan is one coalesced row read by a warp.
 __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                   uint32_t *status, int64_t stage_pairs, int first, int count) {
+                                                   uint32_t *status, float *__restrict__ gmat, int64_t gmat_stride,
+                                                   int first, int count) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_nrec, s_changed;
+    const unsigned FULL = 0xffffffffu;
     const int maxn = bv.max_pins;
     unsigned long long *key = sm;
     int *comp = (int *)(key + maxn);
@@ -221,18 +226,29 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
     int *par = sel + maxn;
     int *mx = par + maxn;
     int *flag = mx + maxn;
-    const int B = blockDim.x, tid = threadIdx.x;
-    float *wsm = (float *)(flag + maxn);  // pair costs, when the net's fit
+    float *wrec = (float *)(flag + maxn);  // costs of a round's recorded edges, in order
+    float *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : wrec + maxn;
+    const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     for (int t = blockIdx.x; t < count; t += gridDim.x) {
         const int net = bv.order[first + t];
         const int n = bv.npin[net];
-        const int64_t P = (int64_t)n * (n - 1) / 2;
+        const long long P = (long long)n * (n - 1) / 2;
         const float *w = cost + bv.pair_ofs[net];
-        if (P <= stage_pairs) {
-            for (int64_t e = tid; e < P; e += B) wsm[e] = __ldg(w + e);
-            w = wsm;
-        }
         int64_t *out = mst + bv.node_ofs[net];
+        {
+            int j, k;
+            pair_decode(tid, j, k);
+            for (long long e = tid; e < P; e += B) {
+                const float c = __ldg(w + e);
+                M[j * n + k] = c;
+                M[k * n + j] = c;
+                k += B;
+                while (k >= j) {
+                    k -= j;
+                    j++;
+                }
+            }
+        }
         for (int v = tid; v < n; v += B) comp[v] = v;
         if (tid == 0) s_nrec = 0;
         float d = 0.0f;
@@ -242,16 +258,18 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
             rounds++;
             for (int v = tid; v < n; v += B) key[v] = ~0ull;
             __syncthreads();
-            for (int v = tid; v < n; v += B) {
+            for (int v = warp; v < n; v += nw) {
                 const int cv = comp[v];
+                const float *row = M + v * n;
                 unsigned long long best = ~0ull;
-                for (int u = 0; u < n; u++) {
-                    if (comp[u] == cv) continue;
-                    const int64_t e = pair_id(v, u);
-                    const unsigned long long kk = cost_key(w[e], (uint32_t)e);
+                for (int u = lane; u < n; u += 32) {
+                    if (u == v || comp[u] == cv) continue;
+                    const unsigned long long kk = cost_key(row[u], (uint32_t)pair_id(v, u));
                     best = kk < best ? kk : best;
                 }
-                if (best != ~0ull) atomicMin(key + cv, best);
+                const uint32_t hi = __reduce_min_sync(FULL, (uint32_t)(best >> 32));
+                const uint32_t lo = __reduce_min_sync(FULL, (uint32_t)(best >> 32) == hi ? (uint32_t)best : ~0u);
+                if (lane == 0 && hi != ~0u) atomicMin(key + cv, ((unsigned long long)hi << 32) | lo);
             }
             __syncthreads();
             for (int v = tid; v < n; v += B) {
@@ -277,22 +295,25 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
                 mx[v] = -1;
             }
             __syncthreads();
-            // recorded edges in ascending root order
+            // recorded edges in ascending root order; their costs summed in
+            // that order (the reference adds best[r] per union)
             {
                 const int chunk = (n + B - 1) / B;
                 const int c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
                 int cnt = 0;
                 for (int v = c0; v < c1; v++) cnt += flag[v];
                 int total;
-                int pos = block_excl_scan(cnt, warp_sums, total) + s_nrec;
+                int pos = block_excl_scan(cnt, warp_sums, total);
                 for (int v = c0; v < c1; v++)
-                    if (flag[v]) out[pos++] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)sel[v];
-                if (tid == 0) {
-                    for (int v = 0; v < n; v++)
-                        if (flag[v]) d += w[(uint32_t)key[v]];
-                }
+                    if (flag[v]) {
+                        out[s_nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)sel[v];
+                        wrec[pos++] = key_cost(key[v]);
+                    }
                 __syncthreads();
-                if (tid == 0) s_nrec += total;
+                if (tid == 0) {
+                    for (int i = 0; i < total; i++) d += wrec[i];
+                    s_nrec += total;
+                }
             }
             // tops of the candidate trees (acyclic once mutual pairs are cut,
             // so depth halves per step; the bound only guards the proof)
@@ -641,6 +662,9 @@ struct MarkVis {
     uint32_t *sum;
     unsigned long long *list;
     int32_t *count;
+    int32_t *capr;
+    float *dlt;
+    const float *lut;
     unsigned long long ent[kEntBuf];
     int n = 0;
     __device__ __forceinline__ void add(int32_t w, uint32_t bits) {
@@ -654,6 +678,16 @@ struct MarkVis {
         if (nb) {
             if (!old) atomicOr(sum + (w >> 5), 1u << (w & 31));
             add(w, nb);
+            // the owner records the cell's cost increment at its current
+            // capacity (bit_util.hpp:87) and takes the unit of demand (:88)
+            uint32_t b = nb;
+            while (b) {
+                const int32_t e = (w << 5) + __ffs(b) - 1;
+                b &= b - 1;
+                const int c = capr[e];
+                dlt[e] = lut_inc(lut, c);
+                capr[e] = c - 1;
+            }
         }
     }
     __device__ __forceinline__ void span(int32_t e0, int cnt) {
@@ -675,13 +709,14 @@ __global__ void __launch_bounds__(256) k_mark5(GridC g, BatchView bv, const int3
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
                                                int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *sum,
                                                unsigned long long *__restrict__ list, int32_t *count,
-                                               uint32_t *status) {
+                                               int32_t *__restrict__ capr, float *__restrict__ dlt,
+                                               const float *__restrict__ lut, uint32_t *status) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < bv.n_nodes; s0 += stride) {
         const int64_t s = s0 + lane;
-        MarkVis vis{mark, sum, list, count};
+        MarkVis vis{mark, sum, list, count, capr, dlt, lut};
         if (s < bv.n_nodes) {
             EdgeRef r;
             const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
@@ -735,14 +770,44 @@ __device__ __forceinline__ void scan_marks(const uint32_t *__restrict__ mark, co
     }
 }
 
+// v += dlt[q] for every marked q in [lo, hi], ascending. Each non-empty mark
+// word's 32 increments come in as eight 16-byte loads issued together; the
+// marked ones are then added in cell order.
+__device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
+                                           const float *__restrict__ dlt, int32_t lo, int32_t hi, float &v) {
+    if (lo > hi) return;
+    const int wlo = lo >> 5, whi = hi >> 5;
+    for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
+        uint32_t sm = __ldg(sum + sw);
+        if (sw == (wlo >> 5)) sm &= 0xffffffffu << (wlo & 31);
+        if (sw == (whi >> 5)) sm &= 0xffffffffu >> (31 - (whi & 31));
+        while (sm) {
+            const int w = (sw << 5) + __ffs(sm) - 1;
+            sm &= sm - 1;
+            uint32_t m = __ldg(mark + w);
+            if (w == wlo) m &= 0xffffffffu << (lo & 31);
+            if (w == whi) m &= 0xffffffffu >> (31 - (hi & 31));
+            if (!m) continue;
+            const float4 *q4 = reinterpret_cast<const float4 *>(dlt + ((int64_t)w << 5));
+            float4 d4[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) d4[i] = q4[i];
+            const float *d = reinterpret_cast<const float *>(d4);
+#pragma unroll
+            for (int b = 0; b < 32; b++)
+                if ((m >> b) & 1u) v += d[b];
+        }
+    }
+}
+
 // For a marked cell at track position p: walk its update path
 // (bit_util.hpp:39-55). The cell owns node i while no other marked cell lies
 // in (p, i-1]; the owner adds the increments of every marked cell of the
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
 __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
-                                                 const uint32_t *__restrict__ sum, const int32_t *__restrict__ capr,
-                                                 const float *__restrict__ lut, float *__restrict__ fen) {
+                                                 const uint32_t *__restrict__ sum, const float *__restrict__ dlt,
+                                                 float *__restrict__ fen) {
     const int z = e / g.XY;
     const int r = e - z * g.XY;
     const int p = (z & 1) ? r % g.Y : r % g.X;
@@ -759,10 +824,7 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
         if (other) break;
         checked = top;
         float v = fen[top];
-        scan_marks(mark, sum, base + i - (i & -i), top, [&](int32_t q) {
-            v += lut_inc(lut, __ldg(capr + q));
-            return true;
-        });
+        sum_marked(mark, sum, dlt, base + i - (i & -i), top, v);
         fen[top] = v;
     }
 }
@@ -773,8 +835,7 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const uint32_t *__restrict__ sum,
-                                                     const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                     float *__restrict__ fen) {
+                                                     const float *__restrict__ dlt, float *__restrict__ fen) {
     __shared__ int sx[8][32];
     __shared__ unsigned long long se[8][32];
     const int cnt = *count;
@@ -805,29 +866,22 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
             const unsigned long long en = se[wib][lo];
             uint32_t m = (uint32_t)en;
             for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, lut, fen);
+            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, dlt, fen);
         }
         __syncwarp();
     }
 }
 
-// demand += 1 for every marked cell; marks (and emptied summary bits)
-// cleared for the next batch
+// marks (and emptied summary bits) cleared for the next batch
 __global__ void k_finalize5(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
-                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum, int32_t *__restrict__ capr) {
+                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum) {
     const int cnt = *count;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const unsigned long long it = list[t];
         const int32_t w = (int32_t)(it >> 32);
-        const uint32_t bits0 = (uint32_t)it;
-        uint32_t bits = bits0;
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            capr[(w << 5) + b] -= 1;
-        }
-        const uint32_t old = atomicAnd(mark + w, ~bits0);
-        if ((old & ~bits0) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
+        const uint32_t bits = (uint32_t)it;
+        const uint32_t old = atomicAnd(mark + w, ~bits);
+        if ((old & ~bits) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
     }
 }
 
