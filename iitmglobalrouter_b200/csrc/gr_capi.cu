@@ -61,7 +61,6 @@ struct gr_ctx {
     uint32_t *d_mark = nullptr, *d_status = nullptr;
     unsigned long long *d_list = nullptr;  // (word, newly set bits) of a batch's marked cells
     uint32_t *d_sum = nullptr;             // one bit per mark word holding any mark
-    float *d_dlt = nullptr;                // cost increment of each cell marked in the batch
     DevBuf mat;                            // per-CTA pair-cost matrices of the largest nets
     int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
@@ -344,15 +343,14 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
     k_mark5<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                           c->d_sum, c->d_list, c->d_list_count, c->d_capr,
-                                                           c->d_dlt, c->d_lut, c->d_status);
+                                                           c->d_sum, c->d_list, c->d_list_count, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
     k_fen_update6<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
-                                                        c->d_dlt, c->d_fen);
+                                                        c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
-    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum);
+    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum, c->d_capr);
     prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -480,10 +478,11 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
-    if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4) || cudaMalloc(&c->d_fen, cell4) ||
+    // capr is read in aligned 32-cell words: pad it to a whole last word
+    if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4 + 128) || cudaMalloc(&c->d_fen, cell4) ||
         cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list, sizeof(unsigned long long) * (size_t)csize) ||
         cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
-        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) || cudaMalloc(&c->d_dlt, cell4 + 128) ||
+        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) || 
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
@@ -520,7 +519,6 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_status);
     cudaFree(c->d_list);
     cudaFree(c->d_sum);
-    cudaFree(c->d_dlt);
     free_buf(c->mat);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);

@@ -6,9 +6,9 @@
 //   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
-//   k_mark5        GCELLs of every MST edge, batch-deduped, demand += 1 (mst_bit_commit.hpp:81-235)
+//   k_mark5        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
 //   k_fen_update6  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize5    marks cleared for the next batch
+//   k_finalize5    demand += 1 per marked cell, marks cleared
 #pragma once
 #include "gr_device.cuh"
 
@@ -662,9 +662,6 @@ struct MarkVis {
     uint32_t *sum;
     unsigned long long *list;
     int32_t *count;
-    int32_t *capr;
-    float *dlt;
-    const float *lut;
     unsigned long long ent[kEntBuf];
     int n = 0;
     __device__ __forceinline__ void add(int32_t w, uint32_t bits) {
@@ -678,16 +675,6 @@ struct MarkVis {
         if (nb) {
             if (!old) atomicOr(sum + (w >> 5), 1u << (w & 31));
             add(w, nb);
-            // the owner records the cell's cost increment at its current
-            // capacity (bit_util.hpp:87) and takes the unit of demand (:88)
-            uint32_t b = nb;
-            while (b) {
-                const int32_t e = (w << 5) + __ffs(b) - 1;
-                b &= b - 1;
-                const int c = capr[e];
-                dlt[e] = lut_inc(lut, c);
-                capr[e] = c - 1;
-            }
         }
     }
     __device__ __forceinline__ void span(int32_t e0, int cnt) {
@@ -709,14 +696,13 @@ __global__ void __launch_bounds__(256) k_mark5(GridC g, BatchView bv, const int3
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
                                                int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *sum,
                                                unsigned long long *__restrict__ list, int32_t *count,
-                                               int32_t *__restrict__ capr, float *__restrict__ dlt,
-                                               const float *__restrict__ lut, uint32_t *status) {
+                                               uint32_t *status) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < bv.n_nodes; s0 += stride) {
         const int64_t s = s0 + lane;
-        MarkVis vis{mark, sum, list, count, capr, dlt, lut};
+        MarkVis vis{mark, sum, list, count};
         if (s < bv.n_nodes) {
             EdgeRef r;
             const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
@@ -770,11 +756,13 @@ __device__ __forceinline__ void scan_marks(const uint32_t *__restrict__ mark, co
     }
 }
 
-// v += dlt[q] for every marked q in [lo, hi], ascending. Each non-empty mark
-// word's 32 increments come in as eight 16-byte loads issued together; the
-// marked ones are then added in cell order.
+// v += cost(cap-1) - cost(cap) of every marked q in [lo, hi], ascending
+// (bit_util.hpp:87-89 with the adds serialised in cell order). Each
+// non-empty mark word's 32 capacities come in as eight 16-byte loads issued
+// together; the marked cells' increments are then added in cell order.
 __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
-                                           const float *__restrict__ dlt, int32_t lo, int32_t hi, float &v) {
+                                           const int32_t *__restrict__ capr, const float *__restrict__ lut,
+                                           int32_t lo, int32_t hi, float &v) {
     if (lo > hi) return;
     const int wlo = lo >> 5, whi = hi >> 5;
     for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
@@ -788,14 +776,17 @@ __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, co
             if (w == wlo) m &= 0xffffffffu << (lo & 31);
             if (w == whi) m &= 0xffffffffu >> (31 - (hi & 31));
             if (!m) continue;
-            const float4 *q4 = reinterpret_cast<const float4 *>(dlt + ((int64_t)w << 5));
-            float4 d4[8];
+            const int4 *q4 = reinterpret_cast<const int4 *>(capr + ((int64_t)w << 5));
+            int4 c4[8];
 #pragma unroll
-            for (int i = 0; i < 8; i++) d4[i] = q4[i];
-            const float *d = reinterpret_cast<const float *>(d4);
+            for (int i = 0; i < 8; i++) c4[i] = __ldg(q4 + i);
+            const int *cc = reinterpret_cast<const int *>(c4);
+            float inc[32];
+#pragma unroll
+            for (int b = 0; b < 32; b++) inc[b] = ((m >> b) & 1u) ? lut_inc(lut, cc[b]) : 0.0f;
 #pragma unroll
             for (int b = 0; b < 32; b++)
-                if ((m >> b) & 1u) v += d[b];
+                if ((m >> b) & 1u) v += inc[b];
         }
     }
 }
@@ -806,8 +797,8 @@ __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, co
 // node's range (i - lowbit(i), i] in ascending cell order. Each node touched
 // by the batch thus has exactly one writer and a fixed summation order.
 __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
-                                                 const uint32_t *__restrict__ sum, const float *__restrict__ dlt,
-                                                 float *__restrict__ fen) {
+                                                 const uint32_t *__restrict__ sum, const int32_t *__restrict__ capr,
+                                                 const float *__restrict__ lut, float *__restrict__ fen) {
     const int z = e / g.XY;
     const int r = e - z * g.XY;
     const int p = (z & 1) ? r % g.Y : r % g.X;
@@ -824,7 +815,7 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
         if (other) break;
         checked = top;
         float v = fen[top];
-        sum_marked(mark, sum, dlt, base + i - (i & -i), top, v);
+        sum_marked(mark, sum, capr, lut, base + i - (i & -i), top, v);
         fen[top] = v;
     }
 }
@@ -835,7 +826,8 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const uint32_t *__restrict__ sum,
-                                                     const float *__restrict__ dlt, float *__restrict__ fen) {
+                                                     const int32_t *__restrict__ capr, const float *__restrict__ lut,
+                                                     float *__restrict__ fen) {
     __shared__ int sx[8][32];
     __shared__ unsigned long long se[8][32];
     const int cnt = *count;
@@ -866,22 +858,29 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
             const unsigned long long en = se[wib][lo];
             uint32_t m = (uint32_t)en;
             for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, dlt, fen);
+            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, lut, fen);
         }
         __syncwarp();
     }
 }
 
-// marks (and emptied summary bits) cleared for the next batch
+// demand += 1 for every marked cell (bit_util.hpp:88); marks and emptied
+// summary bits cleared for the next batch
 __global__ void k_finalize5(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
-                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum) {
+                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum, int32_t *__restrict__ capr) {
     const int cnt = *count;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
         const unsigned long long it = list[t];
         const int32_t w = (int32_t)(it >> 32);
-        const uint32_t bits = (uint32_t)it;
-        const uint32_t old = atomicAnd(mark + w, ~bits);
-        if ((old & ~bits) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
+        const uint32_t bits0 = (uint32_t)it;
+        uint32_t bits = bits0;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            capr[(w << 5) + b] -= 1;
+        }
+        const uint32_t old = atomicAnd(mark + w, ~bits0);
+        if ((old & ~bits0) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
     }
 }
 
