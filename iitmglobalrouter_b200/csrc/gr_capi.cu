@@ -100,6 +100,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
 constexpr int kMstMidPins = 128;         // k_mst_large on 128 threads up to this size
+constexpr int kMstClusterSmem = 227 * 1024;  // dynamic shared memory of k_mst_cluster CTAs
 
 #define GR_CK(call)                                                                            \
     do {                                                                                       \
@@ -267,6 +268,19 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
 size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long long) + 6 * sizeof(int)); }
 // whether a net of n pins keeps its n x n cost matrix in shared memory
 bool mst_mat_in_smem(int n) { return mst_smem(n) + (size_t)n * n * sizeof(float) <= (size_t)kMstSmemMax; }
+// k_mst_cluster shared memory per CTA: partial minima, the block arrays and
+// its ceil(n/cs) matrix rows
+size_t mst_cluster_smem(int n, int cs) {
+    return (size_t)n * sizeof(unsigned long long) + mst_smem(n) + (size_t)((n + cs - 1) / cs) * n * sizeof(float);
+}
+// cluster size for nets of up to n pins (0: no cluster -- one CTA suffices
+// or the matrix needs global memory)
+int mst_cluster_size(int n) {
+    if (n <= kMstMidPins || mst_mat_in_smem(n)) return 0;
+    if (mst_cluster_smem(n, 4) <= (size_t)kMstClusterSmem) return 4;
+    if (mst_cluster_smem(n, 8) <= (size_t)kMstClusterSmem) return 8;
+    return 0;
+}
 
 // ------------------------------------------------------------------ stages
 
@@ -308,29 +322,53 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s, pi, GR_K_MST_WARP);
     }
-    // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above; a
-    // net's full cost matrix sits in shared memory when it fits, else in a
-    // per-CTA global scratch (sized by ensure_mst_scratch)
+    // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above. A
+    // net's full cost matrix sits in the CTA's shared memory when it fits, is
+    // spread over a 4- or 8-CTA cluster when that fits, else goes to a per-CTA
+    // global scratch (sized by ensure_mst_scratch).
     const int nmid = v.nmid, nbig = v.nl - v.nmid;
     for (int part = 0; part < 2; part++) {
         const int cnt = part ? nbig : nmid;
         if (cnt <= 0) continue;
         const int maxn = part ? v.max_pins : (v.max_pins < kMstMidPins ? v.max_pins : kMstMidPins);
-        const bool in_smem = mst_mat_in_smem(maxn);
-        const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
-        int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
-        float *gmat = nullptr;
-        if (!in_smem) {
-            blocks = cnt < c->sm_count ? cnt : c->sm_count;
-            if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
-            gmat = (float *)c->mat.p;
-        }
+        const int first = v.n2 + v.nm + (part ? nmid : 0);
         BatchView vv = v;
         vv.max_pins = maxn;
+        const int cs = mst_cluster_size(maxn);
         int pi = prof_begin(c, s);
-        k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
-                                                          (int64_t)maxn * maxn, v.n2 + v.nm + (part ? nmid : 0),
-                                                          cnt);
+        if (cs) {
+            const int clusters = cnt < c->sm_count / cs ? cnt : c->sm_count / cs;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(clusters * cs);
+            cfg.blockDim = dim3(512);
+            cfg.dynamicSmemBytes = mst_cluster_smem(maxn, cs);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cs;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if (cs == 4)
+                GR_CK(cudaLaunchKernelEx(&cfg, k_mst_cluster<4>, c->g, vv, (const float *)pcost, mst, dist,
+                                         c->d_status, first, cnt));
+            else
+                GR_CK(cudaLaunchKernelEx(&cfg, k_mst_cluster<8>, c->g, vv, (const float *)pcost, mst, dist,
+                                         c->d_status, first, cnt));
+        } else {
+            const bool in_smem = mst_mat_in_smem(maxn);
+            const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
+            int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
+            float *gmat = nullptr;
+            if (!in_smem) {
+                blocks = cnt < c->sm_count ? cnt : c->sm_count;
+                if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
+                gmat = (float *)c->mat.p;
+            }
+            k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
+                                                              (int64_t)maxn * maxn, first, cnt);
+        }
         prof_end(c, s, pi, GR_K_MST_LARGE);
     }
     GR_CK(cudaGetLastError());
@@ -364,7 +402,7 @@ int check_mst_smem(gr_ctx *c, int max_pins) {
 // global pair-cost matrices for k_mst_large when a batch's largest net
 // does not fit in shared memory (one matrix per CTA, at most one CTA per SM)
 int ensure_mst_scratch(gr_ctx *c, int max_pins, cudaStream_t s) {
-    if (max_pins <= kMstMidPins || mst_mat_in_smem(max_pins)) return GR_OK;
+    if (max_pins <= kMstMidPins || mst_mat_in_smem(max_pins) || mst_cluster_size(max_pins)) return GR_OK;
     return ensure(c->mat, (size_t)c->sm_count * max_pins * max_pins * sizeof(float), s);
 }
 
@@ -497,6 +535,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_sum, 0, (words / 32 + 2) * 4))
         return fail(GR_ERR_CUDA);
     c->mst_smem_max = kMstSmemMax;
+    if (cudaFuncSetAttribute(k_mst_cluster<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem) ||
+        cudaFuncSetAttribute(k_mst_cluster<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem))
+        return fail(GR_ERR_CUDA);
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
         cudaSuccess)
         return fail(GR_ERR_CUDA);

@@ -10,7 +10,11 @@
 //   k_fen_update6  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
 //   k_finalize5    demand += 1 per marked cell, marks cleared
 #pragma once
+#include <cooperative_groups.h>
+
 #include "gr_device.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace gr {
 
@@ -208,6 +212,111 @@ __device__ __forceinline__ int64_t pair_id(int a, int b) {
     return a > b ? (int64_t)a * (a - 1) / 2 + b : (int64_t)b * (b - 1) / 2 + a;
 }
 
+// Per-pin state of a block-level Boruvka, in shared memory.
+struct MstArrays {
+    unsigned long long *key;  // per root: min (cost, pair id) of its crossing pairs
+    int *comp, *sel, *par, *mx, *flag;
+    float *wrec;              // costs of a round's recorded edges, in order
+    __device__ static MstArrays carve(void *base, int maxn) {
+        MstArrays a;
+        a.key = (unsigned long long *)base;
+        a.comp = (int *)(a.key + maxn);
+        a.sel = a.comp + maxn;
+        a.par = a.sel + maxn;
+        a.mx = a.par + maxn;
+        a.flag = a.mx + maxn;
+        a.wrec = (float *)(a.flag + maxn);
+        return a;
+    }
+    __device__ float *end(int maxn) const { return wrec + maxn; }
+};
+
+// One pin's scan: min key over its crossing pairs, as a warp (row = the
+// pin's costs to every other pin), posted to its root.
+__device__ __forceinline__ void mst_scan_row(const MstArrays &a, const float *row, int v, int n, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const int cv = a.comp[v];
+    unsigned long long best = ~0ull;
+    for (int u = lane; u < n; u += 32) {
+        if (u == v || a.comp[u] == cv) continue;
+        const unsigned long long kk = cost_key(row[u], (uint32_t)pair_id(v, u));
+        best = kk < best ? kk : best;
+    }
+    const uint32_t hi = __reduce_min_sync(FULL, (uint32_t)(best >> 32));
+    const uint32_t lo = __reduce_min_sync(FULL, (uint32_t)(best >> 32) == hi ? (uint32_t)best : ~0u);
+    if (lane == 0 && hi != ~0u) atomicMin(a.key + cv, ((unsigned long long)hi << 32) | lo);
+}
+
+// The rest of a round once a.key holds every root's minimum (gmst_util.hpp:
+// 215-341): select the other side, record every candidate except the larger
+// root of each mutual pair in ascending root order (written to out when out
+// is not null), sum their costs into d in that order, and merge. A merged
+// component's root is its largest pin index (union points the smaller root
+// at the larger one), found by following each candidate's chain to its
+// tree's top. Returns the number of edges recorded this round.
+__device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net, int nrec, int64_t *out, float &d,
+                                              int *warp_sums, int *s_total, uint32_t *status) {
+    const int B = blockDim.x, tid = threadIdx.x;
+    for (int v = tid; v < n; v += B) {
+        int s = -1;
+        if (a.comp[v] == v && a.key[v] != ~0ull) {
+            int j, k;
+            pair_decode((long long)(uint32_t)a.key[v], j, k);
+            s = (a.comp[j] == v) ? a.comp[k] : a.comp[j];
+        }
+        a.sel[v] = s;
+    }
+    __syncthreads();
+    for (int v = tid; v < n; v += B) {
+        const int s = a.sel[v];
+        if (s >= 0) {
+            const bool mutual_top = (a.sel[s] == v) && (v > s);
+            a.flag[v] = mutual_top ? 0 : 1;
+            a.par[v] = mutual_top ? v : s;
+        } else {
+            a.flag[v] = 0;
+            a.par[v] = v;
+        }
+        a.mx[v] = -1;
+    }
+    __syncthreads();
+    const int chunk = (n + B - 1) / B;
+    const int c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
+    int cnt = 0;
+    for (int v = c0; v < c1; v++) cnt += a.flag[v];
+    int total;
+    int pos = block_excl_scan(cnt, warp_sums, total);
+    for (int v = c0; v < c1; v++)
+        if (a.flag[v]) {
+            if (out) out[nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)a.sel[v];
+            a.wrec[pos++] = key_cost(a.key[v]);
+        }
+    __syncthreads();
+    if (tid == 0) {
+        float dd = d;
+        for (int i = 0; i < total; i++) dd += a.wrec[i];
+        d = dd;
+    }
+    for (int v = tid; v < n; v += B) {
+        if (a.sel[v] < 0) continue;
+        int p = v, steps = 0;
+        while (a.par[p] != p && steps < n) {
+            p = a.par[p];
+            steps++;
+        }
+        if (steps >= n) atomicOr(status, 0x4u);
+        a.flag[v] = p;  // flag[] is free again: it now holds the top
+        atomicMax(a.mx + p, v);
+    }
+    __syncthreads();
+    for (int u = tid; u < n; u += B) {
+        const int r = a.comp[u];
+        if (a.sel[r] >= 0) a.comp[u] = a.mx[a.flag[r]];
+    }
+    __syncthreads();
+    return total;
+}
+
 // The net's pair costs are first spread into a full symmetric n x n matrix
 // (shared memory when it fits, else this CTA's global scratch) so that each
 // pin's crossing scan is one coalesced row read by a warp.
@@ -217,17 +326,10 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
                                                    int first, int count) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
-    __shared__ int s_nrec, s_changed;
-    const unsigned FULL = 0xffffffffu;
+    __shared__ int s_total;
     const int maxn = bv.max_pins;
-    unsigned long long *key = sm;
-    int *comp = (int *)(key + maxn);
-    int *sel = comp + maxn;
-    int *par = sel + maxn;
-    int *mx = par + maxn;
-    int *flag = mx + maxn;
-    float *wrec = (float *)(flag + maxn);  // costs of a round's recorded edges, in order
-    float *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : wrec + maxn;
+    const MstArrays a = MstArrays::carve(sm, maxn);
+    float *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : a.end(maxn);
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     for (int t = blockIdx.x; t < count; t += gridDim.x) {
         const int net = bv.order[first + t];
@@ -249,108 +351,89 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
                 }
             }
         }
-        for (int v = tid; v < n; v += B) comp[v] = v;
-        if (tid == 0) s_nrec = 0;
+        for (int v = tid; v < n; v += B) a.comp[v] = v;
         float d = 0.0f;
-        int rounds = 0;
+        int nrec = 0, rounds = 0;
         __syncthreads();
-        while (s_nrec < n - 1 && rounds < kMstMaxRounds) {
+        while (nrec < n - 1 && rounds < kMstMaxRounds) {
             rounds++;
-            for (int v = tid; v < n; v += B) key[v] = ~0ull;
+            for (int v = tid; v < n; v += B) a.key[v] = ~0ull;
             __syncthreads();
-            for (int v = warp; v < n; v += nw) {
-                const int cv = comp[v];
-                const float *row = M + v * n;
-                unsigned long long best = ~0ull;
-                for (int u = lane; u < n; u += 32) {
-                    if (u == v || comp[u] == cv) continue;
-                    const unsigned long long kk = cost_key(row[u], (uint32_t)pair_id(v, u));
-                    best = kk < best ? kk : best;
-                }
-                const uint32_t hi = __reduce_min_sync(FULL, (uint32_t)(best >> 32));
-                const uint32_t lo = __reduce_min_sync(FULL, (uint32_t)(best >> 32) == hi ? (uint32_t)best : ~0u);
-                if (lane == 0 && hi != ~0u) atomicMin(key + cv, ((unsigned long long)hi << 32) | lo);
-            }
+            for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * n, v, n, lane);
             __syncthreads();
-            for (int v = tid; v < n; v += B) {
-                int s = -1;
-                if (comp[v] == v && key[v] != ~0ull) {
-                    int j, k;
-                    pair_decode((long long)(uint32_t)key[v], j, k);
-                    s = (comp[j] == v) ? comp[k] : comp[j];
-                }
-                sel[v] = s;
-            }
-            __syncthreads();
-            for (int v = tid; v < n; v += B) {
-                int s = sel[v];
-                if (s >= 0) {
-                    bool mutual_top = (sel[s] == v) && (v > s);
-                    flag[v] = mutual_top ? 0 : 1;
-                    par[v] = mutual_top ? v : s;
-                } else {
-                    flag[v] = 0;
-                    par[v] = v;
-                }
-                mx[v] = -1;
-            }
-            __syncthreads();
-            // recorded edges in ascending root order; their costs summed in
-            // that order (the reference adds best[r] per union)
-            {
-                const int chunk = (n + B - 1) / B;
-                const int c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
-                int cnt = 0;
-                for (int v = c0; v < c1; v++) cnt += flag[v];
-                int total;
-                int pos = block_excl_scan(cnt, warp_sums, total);
-                for (int v = c0; v < c1; v++)
-                    if (flag[v]) {
-                        out[s_nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)sel[v];
-                        wrec[pos++] = key_cost(key[v]);
-                    }
-                __syncthreads();
-                if (tid == 0) {
-                    for (int i = 0; i < total; i++) d += wrec[i];
-                    s_nrec += total;
-                }
-            }
-            // tops of the candidate trees (acyclic once mutual pairs are cut,
-            // so depth halves per step; the bound only guards the proof)
-            for (int step = 0;; step++) {
-                if (tid == 0) s_changed = 0;
-                __syncthreads();
-                for (int v = tid; v < n; v += B) {
-                    int p = par[v], pp = par[p];
-                    if (pp != p) {
-                        par[v] = pp;
-                        s_changed = 1;
-                    }
-                }
-                __syncthreads();
-                if (!s_changed) break;
-                if (step >= 64) {
-                    if (tid == 0) atomicOr(status, 0x4u);
-                    break;
-                }
-                __syncthreads();
-            }
-            for (int v = tid; v < n; v += B)
-                if (sel[v] >= 0) atomicMax(mx + par[v], v);
-            __syncthreads();
-            for (int u = tid; u < n; u += B) {
-                int r = comp[u];
-                if (sel[r] >= 0) comp[u] = mx[par[r]];
-            }
-            __syncthreads();
+            nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, &s_total, status);
         }
-        const int nrec = s_nrec;
         for (int v = nrec + tid; v < n; v += B) out[v] = -1;
         if (tid == 0) {
             if (dist) dist[net] = d;
             if (nrec != n - 1) atomicOr(status, 0x4u);
         }
         __syncthreads();
+    }
+}
+
+// Nets whose n x n matrix exceeds one CTA's shared memory: a cluster of CS
+// CTAs holds it row-distributed. Each CTA scans its own rows into its key[],
+// the per-root minima are combined through distributed shared memory, and
+// the rest of the round runs identically in every CTA (rank 0 writes).
+template <int CS>
+__global__ void __launch_bounds__(512) k_mst_cluster(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                     int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                     uint32_t *status, int first, int count) {
+    extern __shared__ unsigned long long sm[];
+    __shared__ int warp_sums[32];
+    __shared__ int s_total;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int maxn = bv.max_pins;
+    unsigned long long *part = sm;  // this CTA's per-root minima over its rows
+    const MstArrays a = MstArrays::carve(part + maxn, maxn);
+    float *M = a.end(maxn);
+    const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
+    const int ncl = gridDim.x / CS, cid = blockIdx.x / CS;
+    for (int t = cid; t < count; t += ncl) {
+        const int net = bv.order[first + t];
+        const int n = bv.npin[net];
+        const int rn = (n + CS - 1) / CS, r0 = min(n, rank * rn), r1 = min(n, r0 + rn);
+        const float *w = cost + bv.pair_ofs[net];
+        for (int idx = tid; idx < (r1 - r0) * n; idx += B) {
+            const int v = r0 + idx / n, u = idx - (v - r0) * n;
+            M[idx] = u == v ? 0.0f : __ldg(w + pair_id(v, u));
+        }
+        for (int v = tid; v < n; v += B) a.comp[v] = v;
+        float d = 0.0f;
+        int nrec = 0, rounds = 0;
+        __syncthreads();
+        while (nrec < n - 1 && rounds < kMstMaxRounds) {
+            rounds++;
+            for (int v = tid; v < n; v += B) part[v] = ~0ull;
+            __syncthreads();
+            const MstArrays ap = {part, a.comp, a.sel, a.par, a.mx, a.flag, a.wrec};
+            for (int v = r0 + warp; v < r1; v += nw) mst_scan_row(ap, M + (int64_t)(v - r0) * n, v, n, lane);
+            cl.sync();  // every CTA's partial minima final
+            for (int v = tid; v < n; v += B) {
+                unsigned long long k = part[v];
+#pragma unroll
+                for (int r = 0; r < CS; r++) {
+                    if (r == rank) continue;
+                    const unsigned long long o = cl.map_shared_rank(part, r)[v];
+                    k = o < k ? o : k;
+                }
+                a.key[v] = k;
+            }
+            cl.sync();  // remote reads done before the partials are reset
+            nrec += mst_round_tail(a, n, net, nrec, rank == 0 ? mst + bv.node_ofs[net] : nullptr, d, warp_sums,
+                                   &s_total, status);
+        }
+        if (rank == 0) {
+            int64_t *out = mst + bv.node_ofs[net];
+            for (int v = nrec + tid; v < n; v += B) out[v] = -1;
+            if (tid == 0) {
+                if (dist) dist[net] = d;
+                if (nrec != n - 1) atomicOr(status, 0x4u);
+            }
+        }
+        cl.sync();
     }
 }
 
@@ -760,9 +843,14 @@ __device__ __forceinline__ void scan_marks(const uint32_t *__restrict__ mark, co
 // (bit_util.hpp:87-89 with the adds serialised in cell order). Each
 // non-empty mark word's 32 capacities come in as eight 16-byte loads issued
 // together; the marked cells' increments are then added in cell order.
+__device__ __forceinline__ float dlut_at(const float *dlut, int c) {
+    c = c < kLutMin ? kLutMin : (c > kLutMax + 1 ? kLutMax + 1 : c);
+    return dlut[c - kLutMin];
+}
+
 __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
-                                           const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                           int32_t lo, int32_t hi, float &v) {
+                                           const int32_t *__restrict__ capr, const float *dlut, int32_t lo,
+                                           int32_t hi, float &v) {
     if (lo > hi) return;
     const int wlo = lo >> 5, whi = hi >> 5;
     for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
@@ -783,7 +871,7 @@ __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, co
             const int *cc = reinterpret_cast<const int *>(c4);
             float inc[32];
 #pragma unroll
-            for (int b = 0; b < 32; b++) inc[b] = ((m >> b) & 1u) ? lut_inc(lut, cc[b]) : 0.0f;
+            for (int b = 0; b < 32; b++) inc[b] = ((m >> b) & 1u) ? dlut_at(dlut, cc[b]) : 0.0f;
 #pragma unroll
             for (int b = 0; b < 32; b++)
                 if ((m >> b) & 1u) v += inc[b];
@@ -798,7 +886,7 @@ __device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, co
 // by the batch thus has exactly one writer and a fixed summation order.
 __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
                                                  const uint32_t *__restrict__ sum, const int32_t *__restrict__ capr,
-                                                 const float *__restrict__ lut, float *__restrict__ fen) {
+                                                 const float *dlut, float *__restrict__ fen) {
     const int z = e / g.XY;
     const int r = e - z * g.XY;
     const int p = (z & 1) ? r % g.Y : r % g.X;
@@ -815,7 +903,7 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
         if (other) break;
         checked = top;
         float v = fen[top];
-        sum_marked(mark, sum, capr, lut, base + i - (i & -i), top, v);
+        sum_marked(mark, sum, capr, dlut, base + i - (i & -i), top, v);
         fen[top] = v;
     }
 }
@@ -830,6 +918,9 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
                                                      float *__restrict__ fen) {
     __shared__ int sx[8][32];
     __shared__ unsigned long long se[8][32];
+    __shared__ float dlut[kLutMax - kLutMin + 2];  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
+    for (int c = threadIdx.x; c < kLutMax - kLutMin + 2; c += blockDim.x) dlut[c] = lut_inc(lut, c + kLutMin);
+    __syncthreads();
     const int cnt = *count;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -858,7 +949,7 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
             const unsigned long long en = se[wib][lo];
             uint32_t m = (uint32_t)en;
             for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, lut, fen);
+            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, dlut, fen);
         }
         __syncwarp();
     }
