@@ -100,7 +100,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
 constexpr int kMstMidPins = 128;         // k_mst_large on 128 threads up to this size
-constexpr int kMstClusterSmem = 227 * 1024;  // dynamic shared memory of k_mst_cluster CTAs
+constexpr int kMstClusterSmem = 216 * 1024;  // dynamic shared memory of k_mst_cluster CTAs
 
 #define GR_CK(call)                                                                            \
     do {                                                                                       \
@@ -507,6 +507,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     c->csize = csize;
     int rc = GR_OK;
     auto fail = [&](int code) {
+        const cudaError_t e = cudaGetLastError();
+        if (code == GR_ERR_CUDA && e != cudaSuccess)
+            fprintf(stderr, "iitmgr_b200: gr_create: %s\n", cudaGetErrorString(e));
         gr_destroy(c);
         return code;
     };
@@ -535,6 +538,12 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_sum, 0, (words / 32 + 2) * 4))
         return fail(GR_ERR_CUDA);
     c->mst_smem_max = kMstSmemMax;
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
+        optin < kMstClusterSmem + 1024 || optin < kMstSmemMax + 1024) {
+        fprintf(stderr, "iitmgr_b200: device allows %d bytes of shared memory per block\n", optin);
+        return fail(GR_ERR_CUDA);
+    }
     if (cudaFuncSetAttribute(k_mst_cluster<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem) ||
         cudaFuncSetAttribute(k_mst_cluster<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem))
         return fail(GR_ERR_CUDA);
