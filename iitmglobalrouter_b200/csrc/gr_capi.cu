@@ -83,6 +83,7 @@ struct gr_ctx {
     GraphCache graph;
     int64_t launches = 0;
     int mst_smem_max = 0;
+    int levels = 0;  // nodes on the longest Fenwick update path: 1 + floor(log2(max(X, Y)))
     // optional per-kernel timing (CUDA events around every launch)
     bool profiling = false;
     std::vector<cudaEvent_t> ev;
@@ -380,12 +381,13 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     if (v.n_nodes <= 0) return GR_OK;
     GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
-    k_mark5<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                           c->d_sum, c->d_list, c->d_list_count, c->d_status);
+    k_mark6<<<grid_for(c, v.n_nodes * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat,
+                                                                c->d_mark, c->d_sum, c->d_list, c->d_list_count,
+                                                                c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update6<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
-                                                        c->d_capr, c->d_lut, c->d_fen);
+    k_fen_update7<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
+                                                        c->d_capr, c->d_lut, c->d_fen, c->levels);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);
     k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum, c->d_capr);
@@ -505,6 +507,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     c->g.npat = Z * c->g.Z2;
     c->g.XY = X * Y;
     c->csize = csize;
+    for (int L = X > Y ? X : Y; L > 0; L >>= 1) c->levels++;
     int rc = GR_OK;
     auto fail = [&](int code) {
         const cudaError_t e = cudaGetLastError();

@@ -772,21 +772,67 @@ struct MarkVis {
     __device__ __forceinline__ void cell(int32_t e) { word(e >> 5, 1u << (e & 31)); }
 };
 
-// One thread per MST slot: mark the GCELLs of its edge, then append its
-// entries contiguously (one warp scan and one atomic per warp), so the cells
-// of a path stay together in the list.
-__global__ void __launch_bounds__(256) k_mark5(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+// The marking units of one edge's path: each via cell, and each 32-cell mark
+// word a wire covers (with the word's bits inside the wire).
+// A path has at most three layer changes of up to Z-2 interior cells and two
+// wires.
+constexpr int kPathSegs = 3 * kMaxLayers + 2;
+struct PathUnits {
+    int seg_n;                    // set to 0 before the walk
+    int seg_kind[kPathSegs];      // 0: via cell, 1: wire
+    int32_t seg_a[kPathSegs];     // via: cell id; wire: first cell id
+    int seg_b[kPathSegs];         // wire: cell count
+    int seg_u[kPathSegs + 1];     // prefix of unit counts
+    __device__ void cell(int32_t e) {
+        seg_kind[seg_n] = 0;
+        seg_a[seg_n] = e;
+        seg_b[seg_n] = 1;
+        seg_u[seg_n + 1] = seg_u[seg_n] + 1;
+        seg_n++;
+    }
+    __device__ void span(int32_t e0, int cnt) {
+        seg_kind[seg_n] = 1;
+        seg_a[seg_n] = e0;
+        seg_b[seg_n] = cnt;
+        seg_u[seg_n + 1] = seg_u[seg_n] + ((e0 + cnt - 1) >> 5) - (e0 >> 5) + 1;
+        seg_n++;
+    }
+    // word and mask of unit u
+    __device__ void unit(int u, int &w, uint32_t &m) const {
+        int s = 0;
+        while (seg_u[s + 1] <= u) s++;
+        const int k = u - seg_u[s];
+        if (seg_kind[s] == 0) {
+            w = seg_a[s] >> 5;
+            m = 1u << (seg_a[s] & 31);
+            return;
+        }
+        const int32_t e0 = seg_a[s], e1 = e0 + seg_b[s] - 1;
+        w = (e0 >> 5) + k;
+        m = 0xffffffffu;
+        if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
+        if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
+    }
+};
+
+// One warp per MST slot: lane 0 lays out the edge's path units, the lanes
+// set their units' marks in parallel, and the (word, newly set bits) entries
+// are appended contiguously with one atomic per edge.
+__global__ void __launch_bounds__(256) k_mark6(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
                                                int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *sum,
                                                unsigned long long *__restrict__ list, int32_t *count,
                                                uint32_t *status) {
+    __shared__ PathUnits su[8];
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t s0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < bv.n_nodes; s0 += stride) {
-        const int64_t s = s0 + lane;
-        MarkVis vis{mark, sum, list, count};
-        if (s < bv.n_nodes) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    PathUnits &pu = su[wib];
+    for (int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; s < bv.n_nodes; s += nwarps) {
+        int units = 0;
+        if (lane == 0) {
+            pu.seg_n = 0;
+            pu.seg_u[0] = 0;
             EdgeRef r;
             const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
             if (ok <= 0) {
@@ -794,21 +840,33 @@ __global__ void __launch_bounds__(256) k_mark5(GridC g, BatchView bv, const int3
                 if (ok < 0) atomicOr(status, 0x1u);
             } else {
                 if (mst_pat) mst_pat[s] = r.cpat;
-                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, vis)) atomicOr(status, 0x2u);
+                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, pu)) atomicOr(status, 0x2u);
+            }
+            units = pu.seg_u[pu.seg_n];
+        }
+        units = __shfl_sync(FULL, units, 0);
+        __syncwarp();
+        int base = 0;
+        for (int u0 = 0; u0 < units; u0 += 32) {
+            const int u = u0 + lane;
+            int w = 0;
+            uint32_t nb = 0;
+            if (u < units) {
+                uint32_t m;
+                pu.unit(u, w, m);
+                const uint32_t old = atomicOr(mark + w, m);
+                nb = m & ~old;
+                if (nb && !old) atomicOr(sum + (w >> 5), 1u << (w & 31));
+            }
+            const unsigned want = __ballot_sync(FULL, nb != 0);
+            if (want) {
+                if (lane == 0) base = atomicAdd(count, __popc(want));
+                base = __shfl_sync(FULL, base, 0);
+                if (nb)
+                    list[base + __popc(want & ((1u << lane) - 1))] = ((unsigned long long)(uint32_t)w << 32) | nb;
             }
         }
         __syncwarp();
-        int incl = vis.n;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int total = __shfl_sync(FULL, incl, 31);
-        int base = 0;
-        if (lane == 31 && total) base = atomicAdd(count, total);
-        base = __shfl_sync(FULL, base, 31) + incl - vis.n;
-        for (int t = 0; t < vis.n; t++) list[base + t] = vis.ent[t];
     }
 }
 
@@ -908,14 +966,17 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
     }
 }
 
-// Each warp takes 32 list entries, prefix-sums their bit counts and hands the
-// cells out one per lane.
-__global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned long long *__restrict__ list,
+// One thread per (marked cell, level of its update path). Level l of the
+// path of position p is node i_l (i_0 = p+1, i_{l+1} = i_l + lowbit(i_l));
+// the cell owns it when no other marked cell lies in (p, i_l - 1] -- a test
+// that needs no lower level, so all levels of a cell proceed in parallel.
+// Each warp takes 32 list entries and deals out their (cell, level) items.
+__global__ void __launch_bounds__(256) k_fen_update7(GridC g, const unsigned long long *__restrict__ list,
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const uint32_t *__restrict__ sum,
                                                      const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                     float *__restrict__ fen) {
+                                                     float *__restrict__ fen, int levels) {
     __shared__ int sx[8][32];
     __shared__ unsigned long long se[8][32];
     __shared__ float dlut[kLutMax - kLutMin + 2];  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
@@ -935,21 +996,39 @@ __global__ void __launch_bounds__(256) k_fen_update6(GridC g, const unsigned lon
             const int y = __shfl_up_sync(FULL, incl, o);
             if (lane >= o) incl += y;
         }
-        const int total = __shfl_sync(FULL, incl, 31);
+        const int total = __shfl_sync(FULL, incl, 31) * levels;
         sx[wib][lane] = incl - c;
         se[wib][lane] = it;
         __syncwarp();
         for (int t = lane; t < total; t += 32) {
-            int lo = 0, hi = 31;  // last entry whose exclusive prefix is <= t
+            const int ci = t / levels, lv = t - ci * levels;
+            int lo = 0, hi = 31;  // last entry whose exclusive prefix is <= ci
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (sx[wib][mid] <= t) lo = mid;
+                if (sx[wib][mid] <= ci) lo = mid;
                 else hi = mid - 1;
             }
             const unsigned long long en = se[wib][lo];
             uint32_t m = (uint32_t)en;
-            for (int q = t - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            fen_owner_update(g, ((int32_t)(en >> 32) << 5) + __ffs(m) - 1, mark, sum, capr, dlut, fen);
+            for (int q = ci - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
+            const int32_t e = ((int32_t)(en >> 32) << 5) + __ffs(m) - 1;
+            const int z = e / g.XY;
+            const int r = e - z * g.XY;
+            const int p = (z & 1) ? r % g.Y : r % g.X;
+            const int L = (z & 1) ? g.Y : g.X;
+            int i = p + 1;
+            for (int k = 0; k < lv; k++) i += i & -i;
+            if (i > L) continue;
+            const int32_t base = e - p, top = base + i - 1;
+            bool other = false;
+            scan_marks(mark, sum, e + 1, top, [&](int32_t) {
+                other = true;
+                return false;
+            });
+            if (other) continue;
+            float v = fen[top];
+            sum_marked(mark, sum, capr, dlut, base + i - (i & -i), top, v);
+            fen[top] = v;
         }
         __syncwarp();
     }
