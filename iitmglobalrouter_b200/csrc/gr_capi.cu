@@ -386,7 +386,7 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
                                                                 c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update7<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
+    k_fen_update8<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
                                                         c->d_capr, c->d_lut, c->d_fen, c->levels);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     pi = prof_begin(c, s);

@@ -969,16 +969,18 @@ __device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, cons
 // One thread per (marked cell, level of its update path). Level l of the
 // path of position p is node i_l (i_0 = p+1, i_{l+1} = i_l + lowbit(i_l));
 // the cell owns it when no other marked cell lies in (p, i_l - 1] -- a test
-// that needs no lower level, so all levels of a cell proceed in parallel.
-// Each warp takes 32 list entries and deals out their (cell, level) items.
-__global__ void __launch_bounds__(256) k_fen_update7(GridC g, const unsigned long long *__restrict__ list,
+// that needs no lower level, so all levels proceed in parallel. Level 0 is
+// always owned; levels >= 1 can only be owned when cell p+1 is unmarked, so
+// only such "span ends" get them. A warp takes up to 32 list entries (fewer
+// when the list is short) and deals out their (cell, level) items.
+__global__ void __launch_bounds__(256) k_fen_update8(GridC g, const unsigned long long *__restrict__ list,
                                                      const int32_t *__restrict__ count,
                                                      const uint32_t *__restrict__ mark,
                                                      const uint32_t *__restrict__ sum,
                                                      const int32_t *__restrict__ capr, const float *__restrict__ lut,
                                                      float *__restrict__ fen, int levels) {
     __shared__ int sx[8][32];
-    __shared__ unsigned long long se[8][32];
+    __shared__ uint32_t sw[8][32], sb[8][32], sends[8][32];
     __shared__ float dlut[kLutMax - kLutMin + 2];  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
     for (int c = threadIdx.x; c < kLutMax - kLutMin + 2; c += blockDim.x) dlut[c] = lut_inc(lut, c + kLutMin);
     __syncthreads();
@@ -986,46 +988,73 @@ __global__ void __launch_bounds__(256) k_fen_update7(GridC g, const unsigned lon
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int e0 = (blockIdx.x * (blockDim.x >> 5) + wib) * 32; e0 < cnt; e0 += warps * 32) {
+    int epw = cnt / warps;  // entries per warp
+    epw = epw < 1 ? 1 : (epw > 32 ? 32 : epw);
+    const int up = levels > 1 ? levels - 1 : 0;  // tracks of one cell have no higher levels
+    for (int e0 = (blockIdx.x * (blockDim.x >> 5) + wib) * epw; e0 < cnt; e0 += warps * epw) {
         const int ei = e0 + lane;
-        const unsigned long long it = ei < cnt ? list[ei] : 0ull;
-        const int c = __popc((uint32_t)it);
+        int c = 0;
+        uint32_t w = 0, bits = 0, ends = 0;
+        if (lane < epw && ei < cnt) {
+            const unsigned long long it = list[ei];
+            w = (uint32_t)(it >> 32);
+            bits = (uint32_t)it;
+            const uint32_t mw = __ldg(mark + w), nx = __ldg(mark + w + 1);
+            ends = bits & ~((mw >> 1) | (nx << 31));  // next cell unmarked
+            c = __popc(bits) + __popc(ends) * up;
+        }
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(FULL, incl, o);
             if (lane >= o) incl += y;
         }
-        const int total = __shfl_sync(FULL, incl, 31) * levels;
+        const int total = __shfl_sync(FULL, incl, 31);
         sx[wib][lane] = incl - c;
-        se[wib][lane] = it;
+        sw[wib][lane] = w;
+        sb[wib][lane] = bits;
+        sends[wib][lane] = ends;
         __syncwarp();
+        const int last = (epw < 32 ? epw : 32) - 1;
         for (int t = lane; t < total; t += 32) {
-            const int ci = t / levels, lv = t - ci * levels;
-            int lo = 0, hi = 31;  // last entry whose exclusive prefix is <= ci
+            int lo = 0, hi = last;  // last entry whose exclusive prefix is <= t
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (sx[wib][mid] <= ci) lo = mid;
+                if (sx[wib][mid] <= t) lo = mid;
                 else hi = mid - 1;
             }
-            const unsigned long long en = se[wib][lo];
-            uint32_t m = (uint32_t)en;
-            for (int q = ci - sx[wib][lo]; q > 0; q--) m &= m - 1;  // drop the lower set bits
-            const int32_t e = ((int32_t)(en >> 32) << 5) + __ffs(m) - 1;
+            int k = t - sx[wib][lo];
+            const uint32_t bb = sb[wib][lo];
+            const int nb = __popc(bb);
+            uint32_t m;
+            int lv;
+            if (k < nb) {
+                m = bb;
+                lv = 0;
+            } else {  // only reached when up > 0
+                k -= nb;
+                m = sends[wib][lo];
+                lv = 1 + k % up;
+                k /= up;
+            }
+            for (; k > 0; k--) m &= m - 1;  // drop the lower set bits
+            const int32_t e = ((int32_t)sw[wib][lo] << 5) + __ffs(m) - 1;
             const int z = e / g.XY;
             const int r = e - z * g.XY;
             const int p = (z & 1) ? r % g.Y : r % g.X;
             const int L = (z & 1) ? g.Y : g.X;
             int i = p + 1;
-            for (int k = 0; k < lv; k++) i += i & -i;
+            for (int q = 0; q < lv; q++) i += i & -i;
             if (i > L) continue;
             const int32_t base = e - p, top = base + i - 1;
-            bool other = false;
-            scan_marks(mark, sum, e + 1, top, [&](int32_t) {
-                other = true;
-                return false;
-            });
-            if (other) continue;
+            if (lv) {
+                bool other = false;
+                scan_marks(mark, sum, e + 1, top, [&](int32_t) {
+                    other = true;
+                    return false;
+                });
+                if (other) continue;
+            }
             float v = fen[top];
             sum_marked(mark, sum, capr, dlut, base + i - (i & -i), top, v);
             fen[top] = v;
