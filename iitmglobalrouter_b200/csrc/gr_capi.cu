@@ -69,12 +69,17 @@ struct gr_ctx {
     std::vector<int64_t> h_pin_ofs;
     int32_t *d_pins = nullptr;
     int32_t *d_pxy = nullptr, *d_cx = nullptr, *d_cy = nullptr;  // per-net coordinate indices and lists
+    int64_t *d_pin_ofs = nullptr;
+    int32_t *d_nxy = nullptr, *d_big = nullptr;
+    size_t nets_cap = 0;
     std::vector<int32_t> h_nxy;                                    // per design net: (nx << 16) | ny
     // per-call batch descriptor (device) + pinned staging
     DevBuf desc, pcost, ppat, tab, dist;
     void *h_stage = nullptr;
     size_t h_stage_bytes = 0;
     cudaEvent_t stage_done = nullptr;
+    cudaStream_t side[3] = {};       // concurrent Boruvka size classes (graph branches when captured)
+    cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
     // plan
     std::vector<BatchInfo> plan;
     DevBuf plan_desc;
@@ -92,8 +97,6 @@ struct gr_ctx {
     double prof_ms[GR_PROF_KINDS] = {};
     int64_t prof_n[GR_PROF_KINDS] = {};
     size_t pins_cap = 0;
-    void *h_coord_pinned = nullptr;  // pinned staging of the coordinate tables
-    size_t coord_cap = 0;
 };
 
 namespace {
@@ -313,15 +316,25 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
 
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s) {
     if (v.n <= 0) return GR_OK;
+    // the size classes are independent: warp and larger-net kernels run on
+    // side streams forked from s and joined back (parallel graph branches)
+    GR_CK(cudaEventRecord(c->ev_fork, s));
+    bool used[3] = {false, false, false};
+    auto side = [&](int i) {
+        if (!used[i]) cudaStreamWaitEvent(c->side[i], c->ev_fork, 0);
+        used[i] = true;
+        return c->side[i];
+    };
     if (v.n2 > 0) {
         int pi = prof_begin(c, s);
         k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
         prof_end(c, s, pi, GR_K_MST);
     }
     if (v.nm > 0) {
-        int pi = prof_begin(c, s);
-        k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s>>>(c->g, v, pcost, mst, dist, c->d_status);
-        prof_end(c, s, pi, GR_K_MST_WARP);
+        cudaStream_t s0 = side(0);
+        int pi = prof_begin(c, s0);
+        k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s0>>>(c->g, v, pcost, mst, dist, c->d_status);
+        prof_end(c, s0, pi, GR_K_MST_WARP);
     }
     // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above. A
     // net's full cost matrix sits in the CTA's shared memory when it fits, is
@@ -336,14 +349,15 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         BatchView vv = v;
         vv.max_pins = maxn;
         const int cs = mst_cluster_size(maxn);
-        int pi = prof_begin(c, s);
+        cudaStream_t sp = side(1 + part);
+        int pi = prof_begin(c, sp);
         if (cs) {
             const int clusters = cnt < c->sm_count / cs ? cnt : c->sm_count / cs;
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(clusters * cs);
             cfg.blockDim = dim3(512);
             cfg.dynamicSmemBytes = mst_cluster_smem(maxn, cs);
-            cfg.stream = s;
+            cfg.stream = sp;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
             attr[0].val.clusterDim.x = cs;
@@ -367,11 +381,16 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
                 if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
                 gmat = (float *)c->mat.p;
             }
-            k_mst_large<<<blocks, part ? 512 : 128, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
+            k_mst_large<<<blocks, part ? 512 : 128, sm, sp>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
                                                               (int64_t)maxn * maxn, first, cnt);
         }
-        prof_end(c, s, pi, GR_K_MST_LARGE);
+        prof_end(c, sp, pi, GR_K_MST_LARGE);
     }
+    for (int i = 0; i < 3; i++)
+        if (used[i]) {
+            GR_CK(cudaEventRecord(c->ev_join[i], c->side[i]));
+            GR_CK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
+        }
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -520,6 +539,11 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         return fail(GR_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GR_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
+    for (int i = 0; i < 3; i++)
+        if (cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
+            return fail(GR_ERR_CUDA);
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
     // capr is read in aligned 32-cell words: pad it to a whole last word
@@ -547,6 +571,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         fprintf(stderr, "iitmgr_b200: device allows %d bytes of shared memory per block\n", optin);
         return fail(GR_ERR_CUDA);
     }
+    if (cudaFuncSetAttribute(k_coords_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 16 * GR_MAX_PINS))
+        return fail(GR_ERR_CUDA);
     if (cudaFuncSetAttribute(k_mst_cluster<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem) ||
         cudaFuncSetAttribute(k_mst_cluster<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem))
         return fail(GR_ERR_CUDA);
@@ -585,9 +611,16 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->dist);
     free_buf(c->plan_desc);
     if (c->h_stage) cudaFreeHost(c->h_stage);
-    if (c->h_coord_pinned) cudaFreeHost(c->h_coord_pinned);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     if (c->stage_done) cudaEventDestroy(c->stage_done);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    for (int i = 0; i < 3; i++) {
+        if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
+        if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
+    }
+    cudaFree(c->d_pin_ofs);
+    cudaFree(c->d_nxy);
+    cudaFree(c->d_big);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GR_OK;
@@ -632,55 +665,52 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
         c->pins_cap = (size_t)(total + 1);
     }
     // per net: sorted distinct x and y coordinates and each pin's index into
-    // them (the query tables are laid out over these coordinates)
-    c->h_nxy.assign(n_nets, 0);
-    if ((size_t)(3 * total + 3) > c->coord_cap) {
-        if (c->h_coord_pinned) cudaFreeHost(c->h_coord_pinned);
-        c->h_coord_pinned = nullptr;
-        c->coord_cap = 0;
-        if (cudaMallocHost(&c->h_coord_pinned, sizeof(int32_t) * (3 * total + 3)) != cudaSuccess) {
+    // them (the query tables are laid out over these coordinates), computed
+    // on the device; only the per-net table shape comes back
+    if ((size_t)(n_nets + 1) > c->nets_cap) {
+        for (void **p : {(void **)&c->d_pin_ofs, (void **)&c->d_nxy, (void **)&c->d_big}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        c->nets_cap = 0;
+        if (cudaMalloc(&c->d_pin_ofs, sizeof(int64_t) * (n_nets + 1)) != cudaSuccess ||
+            cudaMalloc(&c->d_nxy, sizeof(int32_t) * (n_nets + 1)) != cudaSuccess ||
+            cudaMalloc(&c->d_big, sizeof(int32_t) * (n_nets + 1)) != cudaSuccess) {
             cudaGetLastError();
             return GR_ERR_NOMEM;
         }
-        c->coord_cap = (size_t)(3 * total + 3);
+        c->nets_cap = (size_t)(n_nets + 1);
     }
-    int32_t *hp = (int32_t *)c->h_coord_pinned, *hx = hp + total, *hy = hx + total;
-    const int X = c->g.X, Y = c->g.Y, XY = c->g.XY;
-#pragma omp parallel
-    {
-        std::vector<int32_t> xs, ys;
-#pragma omp for schedule(dynamic, 2048)
-        for (int32_t i = 0; i < n_nets; i++) {
-            const int64_t o = h_pin_ofs[i];
-            const int n = (int)(h_pin_ofs[i + 1] - o);
-            xs.resize(n);
-            ys.resize(n);
-            for (int a = 0; a < n; a++) {
-                const int32_t e = h_pins[o + a];
-                const int z = e / XY, r = e - z * XY;
-                xs[a] = (z & 1) ? r / Y : r % X;
-                ys[a] = (z & 1) ? r % Y : r / X;
-            }
-            std::vector<int32_t> ux(xs), uy(ys);
-            std::sort(ux.begin(), ux.end());
-            ux.erase(std::unique(ux.begin(), ux.end()), ux.end());
-            std::sort(uy.begin(), uy.end());
-            uy.erase(std::unique(uy.begin(), uy.end()), uy.end());
-            for (int a = 0; a < n; a++) {
-                const int xi = (int)(std::lower_bound(ux.begin(), ux.end(), xs[a]) - ux.begin());
-                const int yi = (int)(std::lower_bound(uy.begin(), uy.end(), ys[a]) - uy.begin());
-                hp[o + a] = (xi << 16) | yi;
-                hx[o + a] = a < (int)ux.size() ? ux[a] : 0;
-                hy[o + a] = a < (int)uy.size() ? uy[a] : 0;
-            }
-            const int64_t cells = (int64_t)ux.size() * uy.size();
-            c->h_nxy[i] = cells <= kTableMaxCells ? (int32_t)((ux.size() << 16) | uy.size()) : 0;
+    std::vector<int32_t> big;
+    int32_t big_max = 0;
+    for (int32_t i = 0; i < n_nets; i++) {
+        const int32_t k = (int32_t)(h_pin_ofs[i + 1] - h_pin_ofs[i]);
+        if (k > 32) {
+            big.push_back(i);
+            big_max = k > big_max ? k : big_max;
         }
     }
     GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
-    GR_CK(cudaMemcpyAsync(c->d_pxy, hp, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
-    GR_CK(cudaMemcpyAsync(c->d_cx, hx, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
-    GR_CK(cudaMemcpyAsync(c->d_cy, hy, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->d_pin_ofs, h_pin_ofs, sizeof(int64_t) * (n_nets + 1), cudaMemcpyHostToDevice,
+                          c->stream));
+    if (!big.empty())
+        GR_CK(cudaMemcpyAsync(c->d_big, big.data(), sizeof(int32_t) * big.size(), cudaMemcpyHostToDevice,
+                              c->stream));
+    if (n_nets > 0) {
+        k_coords_warp<<<(int)(((int64_t)n_nets * 32 + 255) / 256), 256, 0, c->stream>>>(
+            c->g, n_nets, c->d_pin_ofs, c->d_pins, c->d_pxy, c->d_cx, c->d_cy, c->d_nxy);
+        c->launches++;
+    }
+    if (!big.empty()) {
+        k_coords_block<<<(int)big.size(), 256, 16 * (size_t)big_max, c->stream>>>(
+            c->g, c->d_big, c->d_pin_ofs, c->d_pins, c->d_pxy, c->d_cx, c->d_cy, c->d_nxy);
+        c->launches++;
+    }
+    GR_CK(cudaGetLastError());
+    c->h_nxy.resize(n_nets);
+    if (n_nets > 0)
+        GR_CK(cudaMemcpyAsync(c->h_nxy.data(), c->d_nxy, sizeof(int32_t) * n_nets, cudaMemcpyDeviceToHost,
+                              c->stream));
     c->h_pin_ofs.assign(h_pin_ofs, h_pin_ofs + n_nets + 1);
     c->n_nets = n_nets;
     c->plan.clear();
@@ -759,11 +789,16 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     char *host = (char *)c->h_stage;
     std::vector<BatchInfo> plan(n_batches);
     int64_t slot = 0, mp = 0, mt = 0, mn = 0;
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : bad)
     for (int32_t b = 0; b < n_batches; b++) {
-        int rc = fill_desc(c, h_net_ids + h_batch_ofs[b], (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]),
-                           host, total, h_batch_ofs[b], plan[b]);
-        if (rc) return rc;
-        if ((rc = check_mst_smem(c, plan[b].max_pins))) return rc;
+        int rc = fill_desc(c, h_net_ids + h_batch_ofs[b], (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]), host,
+                           total, h_batch_ofs[b], plan[b]);
+        if (!rc) rc = check_mst_smem(c, plan[b].max_pins);
+        if (rc) bad |= 1 << (-rc);
+    }
+    if (bad) return (bad & (1 << -GR_ERR_NET_TOO_LARGE)) ? GR_ERR_NET_TOO_LARGE : GR_ERR_ARG;
+    for (int32_t b = 0; b < n_batches; b++) {
         plan[b].slot0 = slot;
         slot += plan[b].n_nodes;
         if (plan[b].n_pairs > mp) mp = plan[b].n_pairs;

@@ -44,6 +44,91 @@ struct Coords {
     const int32_t *cy;
 };
 
+// ---------------------------------------------------------------- coordinate tables
+// Per net: the sorted distinct x and y coordinates of its pins and each pin's
+// index into them (nxy[net] = (nx << 16) | ny, 0 when the table would exceed
+// kTableMaxCells). Nets of up to 32 pins: one warp each, pin = lane.
+__global__ void __launch_bounds__(256) k_coords_warp(GridC g, int32_t n_nets, const int64_t *__restrict__ pin_ofs,
+                                                     const int32_t *__restrict__ pins, int32_t *__restrict__ pxy,
+                                                     int32_t *__restrict__ cx, int32_t *__restrict__ cy,
+                                                     int32_t *__restrict__ nxy) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= n_nets) return;
+    const int64_t o = pin_ofs[warp];
+    const int n = (int)(pin_ofs[warp + 1] - o);
+    if (n > 32) return;
+    int x = 0x7fffffff, y = 0x7fffffff;  // lanes past the net sort last and are never counted
+    if (lane < n) {
+        int z;
+        dec(g, pins[o + lane], z, x, y);
+    }
+    const bool fx = (__ffs(__match_any_sync(FULL, x)) - 1) == lane && lane < n;
+    const bool fy = (__ffs(__match_any_sync(FULL, y)) - 1) == lane && lane < n;
+    int xi = 0, yi = 0;
+    for (int b = 0; b < n; b++) {
+        const int xb = __shfl_sync(FULL, x, b), yb = __shfl_sync(FULL, y, b);
+        const bool fxb = __shfl_sync(FULL, fx, b), fyb = __shfl_sync(FULL, fy, b);
+        xi += fxb && xb < x;
+        yi += fyb && yb < y;
+    }
+    const int nx = __popc(__ballot_sync(FULL, fx)), ny = __popc(__ballot_sync(FULL, fy));
+    if (lane < n) {
+        pxy[o + lane] = (xi << 16) | yi;
+        if (fx) cx[o + xi] = x;
+        if (fy) cy[o + yi] = y;
+    }
+    if (lane == 0) nxy[warp] = (int64_t)nx * ny <= kTableMaxCells ? (nx << 16) | ny : 0;
+}
+
+// Larger nets: one CTA each (listed in ids), O(n^2) rank counting in shared
+// memory.
+__global__ void __launch_bounds__(256) k_coords_block(GridC g, const int32_t *__restrict__ ids,
+                                                      const int64_t *__restrict__ pin_ofs,
+                                                      const int32_t *__restrict__ pins, int32_t *__restrict__ pxy,
+                                                      int32_t *__restrict__ cx, int32_t *__restrict__ cy,
+                                                      int32_t *__restrict__ nxy) {
+    extern __shared__ int cs[];
+    __shared__ int s_nx, s_ny;
+    const int net = ids[blockIdx.x];
+    const int64_t o = pin_ofs[net];
+    const int n = (int)(pin_ofs[net + 1] - o);
+    int *xs = cs, *ys = cs + n, *fxs = cs + 2 * n, *fys = cs + 3 * n;
+    if (threadIdx.x == 0) s_nx = s_ny = 0;
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        int z, x, y;
+        dec(g, pins[o + a], z, x, y);
+        xs[a] = x;
+        ys[a] = y;
+    }
+    __syncthreads();
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        bool fx = true, fy = true;
+        for (int b = 0; b < a; b++) {
+            fx &= xs[b] != xs[a];
+            fy &= ys[b] != ys[a];
+        }
+        fxs[a] = fx;
+        fys[a] = fy;
+        if (fx) atomicAdd(&s_nx, 1);
+        if (fy) atomicAdd(&s_ny, 1);
+    }
+    __syncthreads();
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        int xi = 0, yi = 0;
+        for (int b = 0; b < n; b++) {
+            xi += fxs[b] && xs[b] < xs[a];
+            yi += fys[b] && ys[b] < ys[a];
+        }
+        pxy[o + a] = (xi << 16) | yi;
+        if (fxs[a]) cx[o + xi] = xs[a];
+        if (fys[a]) cy[o + yi] = ys[a];
+    }
+    if (threadIdx.x == 0)
+        nxy[net] = (int64_t)s_nx * s_ny <= kTableMaxCells ? (s_nx << 16) | s_ny : 0;
+}
+
 __device__ __forceinline__ float lut_cost(const float *__restrict__ lut, int c) {
     c = c < kLutMin ? kLutMin : (c > kLutMax ? kLutMax : c);
     return __ldg(lut + (c - kLutMin));
