@@ -106,6 +106,7 @@ class Clocks:
 
 def make_workload(config, seed):
     import iitmglobalrouter_b200 as gr
+    from iitmglobalrouter_b200 import replicas
 
     d = gr.Design.generate(config, seed=seed)
     bofs, ids = d.batch(4)
@@ -249,19 +250,17 @@ def main():
         barrier()
     launches = R.launch_count - l0
     clocks = clk.summary()
-    total_ms = float(sum(times))
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = replicas.max_over_ranks(float(sum(times)), dist, dev)
     ms_step = total_ms / args.steps
-    value = world * n_nets * args.steps / (total_ms / 1e3)
+    value = replicas.whole_job_rate(n_nets * args.steps, total_ms / 1e3, world)
 
     # quality of the routed design (plain cost)
     demand = R.demand()
     q = d.evaluate(demand)
     mst_h = mst.cpu().numpy()
     pat_h = pat.cpu().numpy()
+    if not replicas.replicas_agree(replicas.digest(mst_h, pat_h, demand), dist, dev):
+        raise SystemExit("replicas routed the design differently")
     wl, vias = d.write_routes(os.devnull, mst_h, pat_h, merge=True, rseg=True, ppatch=True, threads=8)
 
     # per-kernel breakdown: one profiled step (events around each launch)
@@ -304,11 +303,7 @@ def main():
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_times.append(t1 - t0)
-    e2e_t = sum(e2e_times) / len(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_t], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = replicas.max_over_ranks(sum(e2e_times) / len(e2e_times), dist, dev)
     assert np.array_equal(h_mst.numpy(), mst_h), "end-to-end result differs from the resident run"
     h2d = pins.nbytes + (ids.size * 36 + 64)  # design pins + plan descriptor (pin offsets stay on the host)
     d2h = M * 8 + M * 4
@@ -338,7 +333,7 @@ def main():
                      "algorithmic_bytes_per_step": bnet, "dominant_kernel": dominant},
         "kernels": kernels,
         "cpu_baseline": cpu,
-        "e2e": {"value": world * n_nets / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": replicas.whole_job_rate(n_nets, e2e_t, world), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
         "gpu_launches": int(launches),
         "clocks": clocks,

@@ -1,13 +1,19 @@
 // gr_kernels.cuh -- kernels of the routing hot path (sm_100a).
 //
+// Once per design:
+//   k_coords_warp / k_coords_block  sorted distinct x and y of every net's pins
+// Once per route (reset):
+//   k_fen_init     Fenwick nodes from the capacities      (bit_util.hpp:56-74)
 // Per batch:
 //   k_qtable       per-net query tables (exact Fenwick prefix queries)
 //   k_lpat_z<Z>    L-pattern argmin of every pin pair       (bit_util.hpp:119-191)
+//                  (k_lpat_batch for Z > 16, k_lpat_pairs for explicit pair lists)
 //   k_mst_pin2     Boruvka of 2-pin nets, one thread each     (gmst_util.hpp:164-341)
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
-//   k_mark5        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update6  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
+//   k_mst_cluster  Boruvka of nets whose cost matrix needs a 4- or 8-CTA cluster
+//   k_mark6        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
+//   k_fen_update8  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
 //   k_finalize5    demand += 1 per marked cell, marks cleared
 #pragma once
 #include <cooperative_groups.h>
