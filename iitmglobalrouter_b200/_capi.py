@@ -24,6 +24,7 @@ GR_ST_BAD_EDGE, GR_ST_BAD_PATTERN, GR_ST_MST_ROUNDS, GR_ST_BAD_PIN = 0x1, 0x2, 0
 GR_PLAN_GRAPH = 0x1
 GR_WRT_MERGE, GR_WRT_RSEG, GR_WRT_PPATCH = 0x1, 0x2, 0x4
 GR_MAX_PINS = 4096
+GR_STATIC_MAX_NETS, GR_STATIC_MAX_PINS = 65536, 1024
 GR_PROF_KINDS = 10
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
@@ -38,6 +39,7 @@ SIGNATURES = {
     "gr_set_nets": (_I, [_P, C.c_int32, _P, _P]),
     "gr_lpattern": (_I, [_P, _P, _I64, _P, _P, _P]),
     "gr_brvsk_build": (_I, [_P, _P, C.c_int32, _P, _P, _P, _P]),
+    "gr_brvsk_build_static": (_I, [_P, C.c_int32, _P, _P, _P, _P, _P]),
     "gr_mst_bit_commit": (_I, [_P, _P, C.c_int32, _P, _P, _P, _P]),
     "gr_route_batch": (_I, [_P, _P, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "gr_plan_set": (_I, [_P, C.c_int32, _P, _P]),

@@ -987,3 +987,191 @@ const char *gr_kernel_name(int kind) {
 int64_t gr_launch_count(gr_ctx *c) { return c ? c->launches : -1; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// gr_brvsk_build_static: the Boruvka stage with no allocation and no context.
+//
+// Some callers cannot allocate device memory when they need the spanning
+// trees: an engine whose memory pool already holds the device's free memory,
+// or a loop that must not pay the device-wide synchronisation that cudaFree
+// implies. This entry point keeps everything it needs -- the batch's offset
+// tables and, for nets whose pair-cost matrix exceeds shared memory, the
+// per-CTA matrices -- in one file-scope device array of fixed size, so a call
+// launches kernels and copies pin counts, and allocates nothing.
+//
+// The array is one per device. Calls on a device share it and leave their
+// contents behind; each call rewrites the tables it reads and clears the
+// status word before its kernels run. Calls whose work may overlap on the
+// device (on streams with no ordering between them) race on the array and
+// corrupt each other's results: issue them on one stream.
+// ------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB per device
+constexpr int kStaticMaxNets = GR_STATIC_MAX_NETS;         // nets per call
+constexpr int kStaticMaxPins = GR_STATIC_MAX_PINS;         // pins per net
+constexpr int kStaticMaxDevices = 64;
+// layout of the array (offsets in bytes, each a multiple of 256)
+constexpr size_t kSsStatus = 0;                                             // uint32
+constexpr size_t kSsNpin = 256;                                             // int32 [nets]
+constexpr size_t kSsOrder = kSsNpin + sizeof(int32_t) * kStaticMaxNets;     // int32 [nets]
+constexpr size_t kSsPairOfs = kSsOrder + sizeof(int32_t) * kStaticMaxNets;  // int64 [nets]
+constexpr size_t kSsNodeOfs = kSsPairOfs + sizeof(int64_t) * kStaticMaxNets;
+constexpr size_t kSsMat = kSsNodeOfs + sizeof(int64_t) * kStaticMaxNets;    // float matrices
+static_assert(kSsMat % 256 == 0 && kSsMat + sizeof(float) * kStaticMaxPins * kStaticMaxPins <= kStaticScratchBytes,
+              "static Boruvka scratch holds its tables and at least one largest matrix");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_brvsk_scratch[kStaticScratchBytes];
+
+namespace {
+
+// Pair and slot offsets of a batch from its pin counts: one CTA of 1024
+// threads, each scanning a contiguous chunk, 64-bit sums throughout.
+__global__ void __launch_bounds__(1024) k_static_desc(int32_t n, const int32_t *__restrict__ npin,
+                                                      int32_t *__restrict__ order, int64_t *__restrict__ pair_ofs,
+                                                      int64_t *__restrict__ node_ofs) {
+    const unsigned FULL = 0xffffffffu;
+    __shared__ long long wp[32], wn[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int chunk = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
+    long long sp = 0, sn = 0;
+    for (int i = c0; i < c1; i++) {
+        const long long k = npin[i];
+        sp += k * (k - 1) / 2;
+        sn += k;
+    }
+    long long xp = sp, xn = sn;  // inclusive scans within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long yp = __shfl_up_sync(FULL, xp, o), yn = __shfl_up_sync(FULL, xn, o);
+        if (lane >= o) {
+            xp += yp;
+            xn += yn;
+        }
+    }
+    if (lane == 31) {
+        wp[warp] = xp;
+        wn[warp] = xn;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const long long a = lane < nw ? wp[lane] : 0, b = lane < nw ? wn[lane] : 0;
+        long long ia = a, ib = b;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long ya = __shfl_up_sync(FULL, ia, o), yb = __shfl_up_sync(FULL, ib, o);
+            if (lane >= o) {
+                ia += ya;
+                ib += yb;
+            }
+        }
+        if (lane < nw) {
+            wp[lane] = ia - a;
+            wn[lane] = ib - b;
+        }
+    }
+    __syncthreads();
+    long long P = wp[warp] + xp - sp, N = wn[warp] + xn - sn;
+    for (int i = c0; i < c1; i++) {
+        const long long k = npin[i];
+        pair_ofs[i] = P;
+        node_ofs[i] = N;
+        order[i] = i;
+        P += k * (k - 1) / 2;
+        N += k;
+    }
+}
+
+struct StaticDev {
+    unsigned char *base = nullptr;
+    int sms = 0;
+    bool ready = false;
+};
+std::mutex g_static_mu;
+StaticDev g_static_dev[kStaticMaxDevices];
+
+// Once per device, with that device current: the array's address, the SM
+// count, and the kernels' attributes (which also loads them).
+int static_setup(int dev, StaticDev &out) {
+    if (dev < 0 || dev >= kStaticMaxDevices) return GR_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    StaticDev &d = g_static_dev[dev];
+    if (!d.ready) {
+        void *p = nullptr;
+        GR_CK(cudaGetSymbolAddress(&p, g_brvsk_scratch));
+        int sms = 0, optin = 0;
+        GR_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        GR_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (optin < kMstSmemMax + 1024) {
+            fprintf(stderr, "iitmgr_b200: device allows %d bytes of shared memory per block\n", optin);
+            return GR_ERR_CUDA;
+        }
+        GR_CK(cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstSmemMax));
+        cudaFuncAttributes fa;
+        GR_CK(cudaFuncGetAttributes(&fa, k_static_desc));
+        d.base = (unsigned char *)p;
+        d.sms = sms > 0 ? sms : 1;
+        d.ready = true;
+    }
+    out = d;
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, const float *d_pair_cost,
+                                     int64_t *d_mst_edges, float *d_net_dist, uint32_t *d_status, void *stream) {
+    if (n_nets < 0 || n_nets > kStaticMaxNets) return GR_ERR_ARG;
+    if (n_nets == 0) return GR_OK;
+    if (!h_npin || !d_pair_cost || !d_mst_edges) return GR_ERR_ARG;
+    int maxn = 0;
+    for (int32_t i = 0; i < n_nets; i++) {
+        if (h_npin[i] < 0) return GR_ERR_ARG;
+        if (h_npin[i] > kStaticMaxPins) return GR_ERR_NET_TOO_LARGE;
+        maxn = h_npin[i] > maxn ? h_npin[i] : maxn;
+    }
+    int dev = 0;
+    GR_CK(cudaGetDevice(&dev));
+    StaticDev sd;
+    int rc = static_setup(dev, sd);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    uint32_t *st = d_status ? d_status : (uint32_t *)(sd.base + kSsStatus);
+    int32_t *npin = (int32_t *)(sd.base + kSsNpin), *order = (int32_t *)(sd.base + kSsOrder);
+    int64_t *pair_ofs = (int64_t *)(sd.base + kSsPairOfs), *node_ofs = (int64_t *)(sd.base + kSsNodeOfs);
+    GR_CK(cudaMemsetAsync(sd.base + kSsStatus, 0, sizeof(uint32_t), s));
+    GR_CK(cudaMemcpyAsync(npin, h_npin, sizeof(int32_t) * (size_t)n_nets, cudaMemcpyHostToDevice, s));
+    k_static_desc<<<1, 1024, 0, s>>>(n_nets, npin, order, pair_ofs, node_ofs);
+    GR_CK(cudaGetLastError());
+    BatchView v{};
+    v.n = n_nets;
+    v.npin = npin;
+    v.pair_ofs = pair_ofs;
+    v.node_ofs = node_ofs;
+    v.order = order;
+    v.max_pins = maxn;
+    // k_mst_large for every net: the matrix in shared memory when the largest
+    // net's fits, else one matrix per CTA in the array (as many CTAs as the
+    // array holds, at most one per SM)
+    const bool in_smem = mst_mat_in_smem(maxn);
+    const size_t mat = (size_t)maxn * maxn * sizeof(float);
+    const size_t smem = mst_smem(maxn) + (in_smem ? mat : 0);
+    int blocks;
+    float *gmat = nullptr;
+    if (in_smem) {
+        blocks = n_nets < sd.sms * 8 ? n_nets : sd.sms * 8;
+    } else {
+        const size_t fit = (kStaticScratchBytes - kSsMat) / mat;
+        blocks = (int)(fit < (size_t)sd.sms ? fit : (size_t)sd.sms);
+        blocks = n_nets < blocks ? n_nets : blocks;
+        gmat = (float *)(sd.base + kSsMat);
+    }
+    k_mst_large<<<blocks, maxn <= kMstMidPins ? 128 : 512, smem, s>>>(GridC{}, v, d_pair_cost, d_mst_edges,
+                                                                      d_net_dist, st, gmat, (int64_t)maxn * maxn,
+                                                                      0, n_nets);
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}

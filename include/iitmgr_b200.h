@@ -94,6 +94,25 @@ int gr_lpattern(gr_ctx *ctx, const int32_t *d_pairs, int64_t n_pairs, float *d_c
 int gr_brvsk_build(gr_ctx *ctx, const int32_t *h_net_ids, int32_t n_nets, const float *d_pair_cost,
                    int64_t *d_mst_edges, float *d_net_dist, void *stream);
 
+/* brvsk_build without a context and without allocating: for callers whose
+ * device memory is already spoken for (an engine's pool holds it) or that
+ * must not pay the device-wide synchronisation of cudaFree. No counterpart
+ * in the reference. Net b of the batch has h_npin[b] pins (host memory);
+ * d_pair_cost, d_mst_edges and d_net_dist (may be NULL) are laid out and
+ * filled exactly as by gr_brvsk_build. Status bits (GR_ST_MST_ROUNDS) are
+ * ORed into *d_status when it is not NULL. Works on the calling thread's
+ * current device; stream must belong to it (NULL: the legacy stream).
+ * Limits: at most GR_STATIC_MAX_NETS nets, GR_STATIC_MAX_PINS pins per net
+ * (GR_ERR_ARG / GR_ERR_NET_TOO_LARGE beyond). Its scratch is one fixed
+ * 16 MiB device array per device: the first call on a device does the
+ * set-up (finds the array, loads the kernels) and should come before any
+ * stream capture; calls that may overlap on the device race on the array,
+ * so issue them on one stream. */
+#define GR_STATIC_MAX_NETS 65536
+#define GR_STATIC_MAX_PINS 1024
+int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, const float *d_pair_cost, int64_t *d_mst_edges,
+                          float *d_net_dist, uint32_t *d_status, void *stream);
+
 /* mst_bit_commit: mark every GCELL on the chosen L pattern of every MST
  * edge of the batch (deduplicated over the batch), then each marked cell
  * gains one unit of demand and its track's Fenwick tree gains
