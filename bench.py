@@ -106,7 +106,6 @@ class Clocks:
 
 def make_workload(config, seed):
     import iitmglobalrouter_b200 as gr
-    from iitmglobalrouter_b200 import replicas
 
     d = gr.Design.generate(config, seed=seed)
     bofs, ids = d.batch(4)
@@ -191,6 +190,7 @@ def main():
     import torch
 
     import iitmglobalrouter_b200 as gr
+    from iitmglobalrouter_b200 import replicas
 
     dist = None
     if world > 1:

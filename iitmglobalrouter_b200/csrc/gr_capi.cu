@@ -375,11 +375,11 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
             const bool in_smem = mst_mat_in_smem(maxn);
             const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
             int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
-            float *gmat = nullptr;
+            uint32_t *gmat = nullptr;
             if (!in_smem) {
                 blocks = cnt < c->sm_count ? cnt : c->sm_count;
                 if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
-                gmat = (float *)c->mat.p;
+                gmat = (uint32_t *)c->mat.p;
             }
             k_mst_large<<<blocks, part ? 512 : 128, sm, sp>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
                                                               (int64_t)maxn * maxn, first, cnt);
@@ -1160,14 +1160,14 @@ extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, cons
     const size_t mat = (size_t)maxn * maxn * sizeof(float);
     const size_t smem = mst_smem(maxn) + (in_smem ? mat : 0);
     int blocks;
-    float *gmat = nullptr;
+    uint32_t *gmat = nullptr;
     if (in_smem) {
         blocks = n_nets < sd.sms * 8 ? n_nets : sd.sms * 8;
     } else {
         const size_t fit = (kStaticScratchBytes - kSsMat) / mat;
         blocks = (int)(fit < (size_t)sd.sms ? fit : (size_t)sd.sms);
         blocks = n_nets < blocks ? n_nets : blocks;
-        gmat = (float *)(sd.base + kSsMat);
+        gmat = (uint32_t *)(sd.base + kSsMat);
     }
     k_mst_large<<<blocks, maxn <= kMstMidPins ? 128 : 512, smem, s>>>(GridC{}, v, d_pair_cost, d_mst_edges,
                                                                       d_net_dist, st, gmat, (int64_t)maxn * maxn,

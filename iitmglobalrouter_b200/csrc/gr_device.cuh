@@ -58,11 +58,15 @@ __device__ __forceinline__ float fen_query(const float *__restrict__ fen, int32_
 
 // Order-preserving 64-bit key of (cost, pair id): the Boruvka minimum is
 // the smallest cost, ties broken by the lowest pair id.
-__device__ __forceinline__ unsigned long long cost_key(float w, uint32_t e) {
+// order-preserving bits of a cost: a < b as floats iff bits(a) < bits(b)
+__device__ __forceinline__ uint32_t cost_bits(float w) {
     if (w == 0.0f) w = 0.0f;  // -0 == +0 in the reference's comparisons
-    uint32_t u = __float_as_uint(w);
-    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-    return ((unsigned long long)u << 32) | (unsigned long long)e;
+    const uint32_t u = __float_as_uint(w);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ unsigned long long cost_key(float w, uint32_t e) {
+    return ((unsigned long long)cost_bits(w) << 32) | (unsigned long long)e;
 }
 
 // the cost whose key this is (exact inverse of cost_key's order transform)

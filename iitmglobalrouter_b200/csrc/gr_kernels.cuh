@@ -323,19 +323,32 @@ struct MstArrays {
 };
 
 // One pin's scan: min key over its crossing pairs, as a warp (row = the
-// pin's costs to every other pin), posted to its root.
-__device__ __forceinline__ void mst_scan_row(const MstArrays &a, const float *row, int v, int n, int lane) {
+// pin's cost bits to every other pin), posted to its root. Within a row the
+// pair id grows with u, so the minimum (cost, pair id) is the minimum
+// (cost bits, u); the pair id is formed for the winner only.
+__device__ __forceinline__ void mst_scan_row(const MstArrays &a, const uint32_t *row, int v, int n, int lane) {
     const unsigned FULL = 0xffffffffu;
     const int cv = a.comp[v];
-    unsigned long long best = ~0ull;
-    for (int u = lane; u < n; u += 32) {
-        if (u == v || a.comp[u] == cv) continue;
-        const unsigned long long kk = cost_key(row[u], (uint32_t)pair_id(v, u));
-        best = kk < best ? kk : best;
+    uint32_t bb = ~0u;
+    int bu = 0x7fffffff;
+    int u = lane;
+#pragma unroll 1
+    for (; u + 96 < n; u += 128) {
+        const uint32_t c0 = row[u], c1 = row[u + 32], c2 = row[u + 64], c3 = row[u + 96];
+        const int m0 = a.comp[u], m1 = a.comp[u + 32], m2 = a.comp[u + 64], m3 = a.comp[u + 96];
+        if (m0 != cv && c0 < bb) { bb = c0; bu = u; }
+        if (m1 != cv && c1 < bb) { bb = c1; bu = u + 32; }
+        if (m2 != cv && c2 < bb) { bb = c2; bu = u + 64; }
+        if (m3 != cv && c3 < bb) { bb = c3; bu = u + 96; }
     }
-    const uint32_t hi = __reduce_min_sync(FULL, (uint32_t)(best >> 32));
-    const uint32_t lo = __reduce_min_sync(FULL, (uint32_t)(best >> 32) == hi ? (uint32_t)best : ~0u);
-    if (lane == 0 && hi != ~0u) atomicMin(a.key + cv, ((unsigned long long)hi << 32) | lo);
+    for (; u < n; u += 32) {
+        const uint32_t c = row[u];
+        if (a.comp[u] != cv && c < bb) { bb = c; bu = u; }
+    }
+    const uint32_t hi = __reduce_min_sync(FULL, bb);
+    const uint32_t wu = __reduce_min_sync(FULL, bb == hi ? (uint32_t)bu : 0xffffffffu);
+    if (lane == 0 && wu < (uint32_t)n)
+        atomicMin(a.key + cv, ((unsigned long long)hi << 32) | (unsigned long long)(uint32_t)pair_id(v, (int)wu));
 }
 
 // The rest of a round once a.key holds every root's minimum (gmst_util.hpp:
@@ -413,14 +426,14 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
 // pin's crossing scan is one coalesced row read by a warp.
 __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                   uint32_t *status, float *__restrict__ gmat, int64_t gmat_stride,
+                                                   uint32_t *status, uint32_t *__restrict__ gmat, int64_t gmat_stride,
                                                    int first, int count) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_total;
     const int maxn = bv.max_pins;
     const MstArrays a = MstArrays::carve(sm, maxn);
-    float *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : a.end(maxn);
+    uint32_t *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : (uint32_t *)a.end(maxn);
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     for (int t = blockIdx.x; t < count; t += gridDim.x) {
         const int net = bv.order[first + t];
@@ -429,16 +442,26 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
         const float *w = cost + bv.pair_ofs[net];
         int64_t *out = mst + bv.node_ofs[net];
         {
+            // four independent loads in flight per thread, then their stores;
+            // (j, k) steps through the pair ids e, e + B, e + 2B, ...
             int j, k;
             pair_decode(tid, j, k);
-            for (long long e = tid; e < P; e += B) {
-                const float c = __ldg(w + e);
-                M[j * n + k] = c;
-                M[k * n + j] = c;
-                k += B;
-                while (k >= j) {
-                    k -= j;
-                    j++;
+            for (long long e = tid; e < P; e += 4 * (long long)B) {
+                float c[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) c[i] = e + i * B < P ? __ldg(w + e + i * B) : 0.0f;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (e + i * B < P) {
+                        const uint32_t b = cost_bits(c[i]);
+                        M[j * n + k] = b;
+                        M[k * n + j] = b;
+                    }
+                    k += B;
+                    while (k >= j) {
+                        k -= j;
+                        j++;
+                    }
                 }
             }
         }
@@ -479,7 +502,7 @@ __global__ void __launch_bounds__(512) k_mst_cluster(GridC g, BatchView bv, cons
     const int maxn = bv.max_pins;
     unsigned long long *part = sm;  // this CTA's per-root minima over its rows
     const MstArrays a = MstArrays::carve(part + maxn, maxn);
-    float *M = a.end(maxn);
+    uint32_t *M = (uint32_t *)a.end(maxn);
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     const int ncl = gridDim.x / CS, cid = blockIdx.x / CS;
     for (int t = cid; t < count; t += ncl) {
@@ -487,9 +510,19 @@ __global__ void __launch_bounds__(512) k_mst_cluster(GridC g, BatchView bv, cons
         const int n = bv.npin[net];
         const int rn = (n + CS - 1) / CS, r0 = min(n, rank * rn), r1 = min(n, r0 + rn);
         const float *w = cost + bv.pair_ofs[net];
-        for (int idx = tid; idx < (r1 - r0) * n; idx += B) {
-            const int v = r0 + idx / n, u = idx - (v - r0) * n;
-            M[idx] = u == v ? 0.0f : __ldg(w + pair_id(v, u));
+        // this CTA's rows as cost bits; four independent gathers in flight
+        const int cnt = (r1 - r0) * n;
+        for (int i0 = tid; i0 < cnt; i0 += 4 * B) {
+            float c[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int idx = i0 + i * B;
+                const int v = r0 + idx / n, u = idx - (v - r0) * n;
+                c[i] = (idx < cnt && u != v) ? __ldg(w + pair_id(v, u)) : 0.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (i0 + i * B < cnt) M[i0 + i * B] = cost_bits(c[i]);
         }
         for (int v = tid; v < n; v += B) a.comp[v] = v;
         float d = 0.0f;
