@@ -190,7 +190,7 @@ def main():
     import torch
 
     import iitmglobalrouter_b200 as gr
-    from iitmglobalrouter_b200 import replicas
+    from iitmglobalrouter_b200 import replicas, tune
 
     dist = None
     if world > 1:
@@ -210,6 +210,9 @@ def main():
     R = gr.Router(dims["X"], dims["Y"], dims["Z"], cap, device=local)
     R.set_nets(ofs, pins)
     R.plan_set(bofs, ids)
+    tuning = tune.load(tune.key(R))  # launch shapes from the autotuner's cache, if this GPU and Z are in it
+    tune.apply(R, tuning)
+    tuning = {tune.NAMES[p]: R.tune_get(p) for p in tune.NAMES}
     M = R.plan_slots
     mst = torch.empty(M, dtype=torch.int64, device=dev)
     pat = torch.empty(M, dtype=torch.int32, device=dev)
@@ -327,7 +330,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "nets": n_nets, "pins": dims["n_pins"], "pairs": gr.pair_count(ofs, ids),
                    "batches": len(bofs) - 1, "seed": args.seed, "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MB write) before every timed step", "graph": True},
+                   "l2": "flushed (256 MB write) before every timed step", "graph": True, "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "route step (all kernels)",
                      "algorithmic_bytes_per_step": bnet, "dominant_kernel": dominant},

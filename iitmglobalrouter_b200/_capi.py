@@ -26,6 +26,8 @@ GR_WRT_MERGE, GR_WRT_RSEG, GR_WRT_PPATCH = 0x1, 0x2, 0x4
 GR_MAX_PINS = 4096
 GR_STATIC_MAX_NETS, GR_STATIC_MAX_PINS = 65536, 1024
 GR_PROF_KINDS = 10
+GR_TUNE_MST_MID_THREADS, GR_TUNE_MST_BIG_THREADS, GR_TUNE_MST_CLUSTER_THREADS, GR_TUNE_MST_CLUSTER_MIN_PINS = 0, 1, 2, 3
+GR_TUNE_PARAMS = 4
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
 _P, _I, _I64, _U64, _D = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double
@@ -54,6 +56,8 @@ SIGNATURES = {
     "gr_get_fenwick": (_I, [_P, _P]),
     "gr_stream": (_P, [_P]),
     "gr_launch_count": (_I64, [_P]),
+    "gr_tune_set": (_I, [_P, _I, _I]),
+    "gr_tune_get": (_I, [_P, _I, _P]),
     "gr_profile_enable": (_I, [_P, _I]),
     "gr_profile_read": (_I, [_P, _P, _P, _I]),
     "gr_kernel_name": (C.c_char_p, [_I]),

@@ -88,6 +88,7 @@ struct gr_ctx {
     GraphCache graph;
     int64_t launches = 0;
     int mst_smem_max = 0;
+    int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129};  // GR_TUNE_* values (best measured on B200, Z = 10)
     int levels = 0;  // nodes on the longest Fenwick update path: 1 + floor(log2(max(X, Y)))
     // optional per-kernel timing (CUDA events around every launch)
     bool profiling = false;
@@ -279,8 +280,11 @@ size_t mst_cluster_smem(int n, int cs) {
 }
 // cluster size for nets of up to n pins (0: no cluster -- one CTA suffices
 // or the matrix needs global memory)
-int mst_cluster_size(int n) {
-    if (n <= kMstMidPins || mst_mat_in_smem(n)) return 0;
+// (from_pins > 0: nets of at least that many pins use a cluster whenever one
+// fits, even if one CTA could hold the matrix)
+int mst_cluster_size(int n, int from_pins = 0) {
+    if (n <= kMstMidPins) return 0;
+    if (mst_mat_in_smem(n) && !(from_pins > 0 && n >= from_pins)) return 0;
     if (mst_cluster_smem(n, 4) <= (size_t)kMstClusterSmem) return 4;
     if (mst_cluster_smem(n, 8) <= (size_t)kMstClusterSmem) return 8;
     return 0;
@@ -348,14 +352,14 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         const int first = v.n2 + v.nm + (part ? nmid : 0);
         BatchView vv = v;
         vv.max_pins = maxn;
-        const int cs = mst_cluster_size(maxn);
+        const int cs = mst_cluster_size(maxn, c->tune[GR_TUNE_MST_CLUSTER_MIN_PINS]);
         cudaStream_t sp = side(1 + part);
         int pi = prof_begin(c, sp);
         if (cs) {
             const int clusters = cnt < c->sm_count / cs ? cnt : c->sm_count / cs;
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(clusters * cs);
-            cfg.blockDim = dim3(512);
+            cfg.blockDim = dim3(c->tune[GR_TUNE_MST_CLUSTER_THREADS]);
             cfg.dynamicSmemBytes = mst_cluster_smem(maxn, cs);
             cfg.stream = sp;
             cudaLaunchAttribute attr[1];
@@ -381,7 +385,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
                 if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
                 gmat = (uint32_t *)c->mat.p;
             }
-            k_mst_large<<<blocks, part ? 512 : 128, sm, sp>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
+            k_mst_large<<<blocks, c->tune[part ? GR_TUNE_MST_BIG_THREADS : GR_TUNE_MST_MID_THREADS], sm, sp>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
                                                               (int64_t)maxn * maxn, first, cnt);
         }
         prof_end(c, sp, pi, GR_K_MST_LARGE);
@@ -945,6 +949,27 @@ int gr_get_fenwick(gr_ctx *c, float *h_out) {
 }
 
 void *gr_stream(gr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int gr_tune_set(gr_ctx *c, int param, int value) {
+    if (!c || param < 0 || param >= GR_TUNE_PARAMS) return GR_ERR_ARG;
+    if (param == GR_TUNE_MST_CLUSTER_MIN_PINS) {
+        if (value != 0 && (value <= kMstMidPins || value > GR_MAX_PINS)) return GR_ERR_ARG;
+    } else if (value < 64 || value > 1024 || value % 32) {
+        return GR_ERR_ARG;
+    }
+    if (c->tune[param] != value) {
+        GR_CK(cudaStreamSynchronize(c->stream));
+        drop_graph(c);  // a captured plan holds the old launch shapes
+        c->tune[param] = value;
+    }
+    return GR_OK;
+}
+
+int gr_tune_get(gr_ctx *c, int param, int *value) {
+    if (!c || !value || param < 0 || param >= GR_TUNE_PARAMS) return GR_ERR_ARG;
+    *value = c->tune[param];
+    return GR_OK;
+}
 
 int gr_profile_enable(gr_ctx *c, int on) {
     if (!c) return GR_ERR_ARG;

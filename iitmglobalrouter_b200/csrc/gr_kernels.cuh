@@ -424,7 +424,7 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
 // The net's pair costs are first spread into a full symmetric n x n matrix
 // (shared memory when it fits, else this CTA's global scratch) so that each
 // pin's crossing scan is one coalesced row read by a warp.
-__global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
+__global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
                                                    uint32_t *status, uint32_t *__restrict__ gmat, int64_t gmat_stride,
                                                    int first, int count) {
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(512) k_mst_large(GridC g, BatchView bv, const 
 // the per-root minima are combined through distributed shared memory, and
 // the rest of the round runs identically in every CTA (rank 0 writes).
 template <int CS>
-__global__ void __launch_bounds__(512) k_mst_cluster(GridC g, BatchView bv, const float *__restrict__ cost,
+__global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, const float *__restrict__ cost,
                                                      int64_t *__restrict__ mst, float *__restrict__ dist,
                                                      uint32_t *status, int first, int count) {
     extern __shared__ unsigned long long sm[];

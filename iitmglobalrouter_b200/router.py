@@ -207,6 +207,15 @@ class Router:
                                              len(batch_ofs) - 1, ptr(batch_ofs), ptr(net_ids), ptr(mst_out),
                                              ptr(pat_out), 0), "gr_route_design_host")
 
+    # ---------------------------------------------------------- launch shapes
+    def tune_set(self, param: int, value: int):
+        check(self._lib.gr_tune_set(self._h, param, value), "gr_tune_set")
+
+    def tune_get(self, param: int) -> int:
+        v = C.c_int()
+        check(self._lib.gr_tune_get(self._h, param, C.byref(v)), "gr_tune_get")
+        return v.value
+
     # ---------------------------------------------------------- profiling
     def profile(self, on: bool = True):
         check(self._lib.gr_profile_enable(self._h, int(on)))

@@ -177,6 +177,17 @@ int64_t gr_launch_count(gr_ctx *ctx);
 #define GR_K_MST_WARP 8
 #define GR_K_MST_LARGE 9
 #define GR_PROF_KINDS 10
+/* Launch shapes of the Boruvka size classes (results do not depend on them;
+ * the autotuner in iitmglobalrouter_b200/tune.py picks them per GPU and Z). */
+#define GR_TUNE_MST_MID_THREADS 0      /* threads per CTA, nets of 33..128 pins  */
+#define GR_TUNE_MST_BIG_THREADS 1      /* threads per CTA, larger single-CTA nets */
+#define GR_TUNE_MST_CLUSTER_THREADS 2  /* threads per CTA of a cluster            */
+#define GR_TUNE_MST_CLUSTER_MIN_PINS 3 /* nets from this size use a cluster even
+                                          when one CTA could hold them (0: never) */
+#define GR_TUNE_PARAMS 4
+int gr_tune_set(gr_ctx *ctx, int param, int value); /* threads: 64..1024, multiple of 32 */
+int gr_tune_get(gr_ctx *ctx, int param, int *value);
+
 int gr_profile_enable(gr_ctx *ctx, int on);
 int gr_profile_read(gr_ctx *ctx, double *ms, int64_t *launches, int reset);
 const char *gr_kernel_name(int kind);

@@ -124,6 +124,48 @@ def test_brvsk_boundary_bitexact(cuda):
         assert np.array_equal(bits(dist.cpu().numpy()), bits(dist_c))
 
 
+# (mid threads, big threads, cluster threads, cluster from pins)
+TUNINGS = [(128, 256, 256, 0), (1024, 1024, 1024, 129), (256, 512, 512, 200), (64, 64, 64, 0)]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS)
+def test_brvsk_launch_shapes_do_not_change_results(cuda, tuning):
+    """Every Boruvka launch shape gives the oracle's trees bit for bit: nets
+    in the mid class, single-CTA big nets, 4- and 8-CTA clusters and the
+    global-matrix path (700 pins)."""
+    import torch
+
+    X, Y, Z = 48, 48, 4
+    rng = np.random.default_rng(11)
+    sizes = [2, 3, 33, 64, 128, 129, 150, 200, 220, 221, 300, 450, 700] + [int(k) for k in rng.integers(2, 40, 30)]
+    nets = [np.sort(rng.choice(X * Y * 2, size=n, replace=False)).astype(np.int32) for n in sizes]
+    ofs = np.cumsum([0] + sizes).astype(np.int64)
+    pins = np.concatenate(nets)
+    R = gr.Router(X, Y, Z, np.ones(X * Y * Z, np.int32))
+    R.set_nets(ofs, pins)
+    for p, v in enumerate(tuning):
+        R.tune_set(p, v)
+        assert R.tune_get(p) == v
+    ids = rng.permutation(len(sizes)).astype(np.int32)
+    P, M = gr.pair_count(ofs, ids), gr.slot_count(ofs, ids)
+    w = rng.integers(0, 50, size=P).astype(np.float32) * np.float32(0.25)
+    rc, mst_c, dist_c = oracle.brvsk_build(ofs, ids, w, nthreads=NT)
+    assert rc == 0
+    mst = torch.empty(M, dtype=torch.int64, device="cuda")
+    dist = torch.empty(len(ids), dtype=torch.float32, device="cuda")
+    R.brvsk_build(ids, dev(torch, w), mst, dist)
+    R.sync()
+    assert np.array_equal(mst.cpu().numpy(), mst_c)
+    assert np.array_equal(bits(dist.cpu().numpy()), bits(dist_c))
+
+
+def test_tune_rejects_bad_values(cuda):
+    R = gr.Router(8, 8, 3, np.ones(192, np.int32))
+    for p, v in [(0, 48), (0, 2048), (1, 100), (3, 100), (3, 5000), (7, 512)]:
+        with pytest.raises(gr.GRError):
+            R.tune_set(p, v)
+
+
 def test_commit_boundary_bitexact(cuda):
     import torch
 
