@@ -59,8 +59,6 @@ struct gr_ctx {
     int32_t *d_cap0 = nullptr, *d_capr = nullptr;
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
-    unsigned long long *d_list = nullptr;  // (word, newly set bits) of a batch's marked cells
-    uint32_t *d_sum = nullptr;             // one bit per mark word holding any mark
     DevBuf mat;                            // per-CTA pair-cost matrices of the largest nets
     int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
@@ -80,6 +78,14 @@ struct gr_ctx {
     cudaEvent_t stage_done = nullptr;
     cudaStream_t side[3] = {};       // concurrent Boruvka size classes (graph branches when captured)
     cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
+    float *d_dlut = nullptr;  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
+    // tracks that gained marked cells in a batch: bitmap, list of first cells
+    uint32_t *d_tbits = nullptr;
+    int32_t *d_tlist = nullptr;
+    int32_t n_tracks = 0;
+    int track_cap = 0;                         // marked cells per track compacted in shared memory
+    int32_t *d_gpos = nullptr;                 // CSIZE scratch for tracks beyond track_cap (long tracks only)
+    float *d_gdel = nullptr;
     // plan
     std::vector<BatchInfo> plan;
     DevBuf plan_desc;
@@ -292,7 +298,10 @@ int mst_cluster_size(int n, int from_pins = 0) {
 
 // ------------------------------------------------------------------ stages
 
-int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s) {
+// mst (may be null): also write the trees of the batch's 2-pin nets (and
+// their dist), so that launch_mst can skip k_mst_pin2
+int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s,
+                      int64_t *mst = nullptr, float *dist = nullptr) {
     if (v.n_tab > 0) {
         int pi = prof_begin(c, s);
         k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, coords(c), c->d_fen, tab);
@@ -303,13 +312,15 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
         const int grid = grid_for(c, v.n_pairs, 16);
 #define GR_LPAT_Z(ZV)                                                                                 \
     case ZV:                                                                                          \
-        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat); \
+        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat, mst, \
+                                               dist);                                                   \
         break;
         switch (c->g.Z) {
             GR_LPAT_Z(3) GR_LPAT_Z(4) GR_LPAT_Z(5) GR_LPAT_Z(6) GR_LPAT_Z(7) GR_LPAT_Z(8) GR_LPAT_Z(9)
             GR_LPAT_Z(10) GR_LPAT_Z(11) GR_LPAT_Z(12) GR_LPAT_Z(13) GR_LPAT_Z(14) GR_LPAT_Z(15) GR_LPAT_Z(16)
             default:
-                k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat);
+                k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat,
+                                                       mst, dist);
         }
 #undef GR_LPAT_Z
         prof_end(c, s, pi, GR_K_LPAT);
@@ -318,7 +329,8 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
     return GR_OK;
 }
 
-int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s) {
+int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s,
+               bool pin2_done = false) {
     if (v.n <= 0) return GR_OK;
     // the size classes are independent: warp and larger-net kernels run on
     // side streams forked from s and joined back (parallel graph branches)
@@ -329,7 +341,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         used[i] = true;
         return c->side[i];
     };
-    if (v.n2 > 0) {
+    if (v.n2 > 0 && !pin2_done) {
         int pi = prof_begin(c, s);
         k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
         prof_end(c, s, pi, GR_K_MST);
@@ -399,22 +411,27 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
     return GR_OK;
 }
 
+constexpr int kTrackWarps = 8;       // warps per k_track_commit block
+constexpr int kTrackCapMax = 1024;   // marked cells per track kept in shared memory
+
+size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
+
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
                   cudaStream_t s) {
     if (v.n_nodes <= 0) return GR_OK;
     GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
-    k_mark6<<<grid_for(c, v.n_nodes * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat,
-                                                                c->d_mark, c->d_sum, c->d_list, c->d_list_count,
+    k_mark7<<<grid_for(c, v.n_nodes * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
+                                                                c->d_tbits, c->d_tlist, c->d_list_count,
                                                                 c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     pi = prof_begin(c, s);
-    k_fen_update8<<<c->sm_count * 8, kThreads, 0, s>>>(c->g, c->d_list, c->d_list_count, c->d_mark, c->d_sum,
-                                                        c->d_capr, c->d_lut, c->d_fen, c->levels);
+    int64_t blocks = ((int64_t)c->n_tracks + kTrackWarps - 1) / kTrackWarps;
+    if (blocks > (int64_t)c->sm_count * 8) blocks = (int64_t)c->sm_count * 8;
+    k_track_commit<<<(int)blocks, kTrackWarps * 32, track_smem(c->track_cap), s>>>(
+        c->g, c->d_tlist, c->d_list_count, c->d_mark, c->d_tbits, c->d_capr, c->d_dlut, c->d_fen, c->d_gpos,
+        c->d_gdel, c->track_cap);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
-    pi = prof_begin(c, s);
-    k_finalize5<<<c->sm_count * 8, kThreads, 0, s>>>(c->d_list, c->d_list_count, c->d_mark, c->d_sum, c->d_capr);
-    prof_end(c, s, pi, GR_K_FINALIZE);
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
@@ -475,8 +492,8 @@ int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchV
 int route_one(gr_ctx *c, const BatchView &v, int64_t *mst, int32_t *mst_pat, float *dist, float *pcost,
               int16_t *ppat, cudaStream_t s) {
     int rc;
-    if ((rc = launch_lpat_batch(c, v, pcost, ppat, (float2 *)c->tab.p, s))) return rc;
-    if ((rc = launch_mst(c, v, pcost, mst, dist, s))) return rc;
+    if ((rc = launch_lpat_batch(c, v, pcost, ppat, (float2 *)c->tab.p, s, mst, dist))) return rc;
+    if ((rc = launch_mst(c, v, pcost, mst, dist, s, true))) return rc;
     return launch_commit(c, v, mst, ppat, mst_pat, s);
 }
 
@@ -550,12 +567,18 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
             return fail(GR_ERR_CUDA);
     size_t cell4 = sizeof(int32_t) * csize;
     size_t words = (size_t)(csize / 32 + 2);
+    c->n_tracks = ((Z + 1) / 2) * Y + (Z / 2) * X;
+    c->track_cap = (X > Y ? X : Y) < kTrackCapMax ? (X > Y ? X : Y) : kTrackCapMax;
     // capr is read in aligned 32-cell words: pad it to a whole last word
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4 + 128) || cudaMalloc(&c->d_fen, cell4) ||
-        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list, sizeof(unsigned long long) * (size_t)csize) ||
-        cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
-        cudaMalloc(&c->d_sum, (words / 32 + 2) * 4) || 
-        cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1))) {
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1)) ||
+        cudaMalloc(&c->d_dlut, sizeof(float) * (kLutMax - kLutMin + 2)) ||
+        cudaMalloc(&c->d_tbits, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)) ||
+        cudaMalloc(&c->d_tlist, sizeof(int32_t) * (size_t)(c->n_tracks + 1)) ||
+        (c->track_cap < (X > Y ? X : Y) &&
+         (cudaMalloc(&c->d_gpos, sizeof(int32_t) * (size_t)csize) ||
+          cudaMalloc(&c->d_gdel, sizeof(float) * (size_t)csize)))) {
         cudaGetLastError();
         return fail(GR_ERR_NOMEM);
     }
@@ -566,8 +589,14 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
         cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_sum, 0, (words / 32 + 2) * 4))
+        cudaMemset(c->d_list_count, 0, 16) ||
+        cudaMemset(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)))
         return fail(GR_ERR_CUDA);
+    if (cudaFuncSetAttribute(k_track_commit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)track_smem(c->track_cap)) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
+    k_dlut<<<(kLutMax - kLutMin + 2 + 255) / 256, 256, 0, c->stream>>>(c->d_lut, c->d_dlut);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);
     c->mst_smem_max = kMstSmemMax;
     int optin = 0;
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess ||
@@ -598,10 +627,13 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_capr);
     cudaFree(c->d_fen);
     cudaFree(c->d_lut);
+    cudaFree(c->d_dlut);
+    cudaFree(c->d_tbits);
+    cudaFree(c->d_tlist);
+    cudaFree(c->d_gpos);
+    cudaFree(c->d_gdel);
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
-    cudaFree(c->d_list);
-    cudaFree(c->d_sum);
     free_buf(c->mat);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
@@ -635,7 +667,7 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
-    GR_CK(cudaMemsetAsync(c->d_sum, 0, sizeof(uint32_t) * (size_t)(c->csize / 1024 + 2), s));
+    GR_CK(cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s));
     int pi = prof_begin(c, s);
     k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
     prof_end(c, s, pi, GR_K_FEN_INIT);
@@ -894,13 +926,14 @@ int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, co
         free_buf(pat);
         return rc;
     }
-    rc = gr_route_plan(c, 0, n_batches, (int64_t *)mst.p, (int32_t *)pat.p, flags & ~GR_PLAN_GRAPH, nullptr);
+    rc = gr_route_plan(c, 0, n_batches, (int64_t *)mst.p, (int32_t *)pat.p, flags, nullptr);
     if (!rc) {
         cudaMemcpyAsync(h_mst_edges, mst.p, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream);
         if (h_mst_pat) cudaMemcpyAsync(h_mst_pat, pat.p, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream);
         rc = gr_sync(c);
     }
     cudaStreamSynchronize(c->stream);
+    if (c->graph.mst == mst.p) drop_graph(c);  // the captured plan writes into the buffers freed here
     free_buf(mst);
     free_buf(pat);
     return rc;
@@ -1004,7 +1037,7 @@ int gr_profile_read(gr_ctx *c, double *ms, int64_t *launches, int reset) {
 
 const char *gr_kernel_name(int kind) {
     static const char *names[GR_PROF_KINDS] = {"k_fen_init", "k_qtable", "k_lpat",   "k_mst_pin2",  "k_mark",
-                                               "k_fen_update", "k_finalize", "k_lpat_pairs", "k_mst_warp",
+                                               "k_track_commit", "k_finalize", "k_lpat_pairs", "k_mst_warp",
                                                "k_mst_large"};
     return (kind >= 0 && kind < GR_PROF_KINDS) ? names[kind] : "";
 }

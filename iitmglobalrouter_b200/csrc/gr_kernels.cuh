@@ -12,9 +12,10 @@
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
 //   k_mst_cluster  Boruvka of nets whose cost matrix needs a 4- or 8-CTA cluster
-//   k_mark6        GCELLs of every MST edge, batch-deduped    (mst_bit_commit.hpp:81-235)
-//   k_fen_update8  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
-//   k_finalize5    demand += 1 per marked cell, marks cleared
+//   k_mark7        GCELLs of every MST edge, batch-deduped, and the tracks
+//                  they lie on                                (mst_bit_commit.hpp:81-235)
+//   k_track_commit per touched track: demand += 1 per marked cell and the
+//                  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
 #pragma once
 #include <cooperative_groups.h>
 
@@ -146,6 +147,12 @@ __device__ __forceinline__ float lut_inc(const float *__restrict__ lut, int c) {
     return a - b;
 }
 
+// dlut[c - kLutMin] = cost(c-1) - cost(c) for c = kLutMin .. kLutMax+1, once per context
+__global__ void k_dlut(const float *__restrict__ lut, float *__restrict__ dlut) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < kLutMax - kLutMin + 2; c += gridDim.x * blockDim.x)
+        dlut[c] = lut_inc(lut, c + kLutMin);
+}
+
 // ---------------------------------------------------------------- Fenwick build
 // bit_util.hpp:56-74 builds each node by atomically adding every cell's cost
 // along its update path. Here each node is owned by one thread that adds the
@@ -190,10 +197,22 @@ __global__ void k_qtable(GridC g, BatchView bv, Coords cd, const float *__restri
 }
 
 // ---------------------------------------------------------------- L-pattern
+// A 2-pin net's tree is its single pair: written by the L-pattern kernels in
+// the fused route (same slots as k_mst_pin2: root 0 records (0, 1)).
+__device__ __forceinline__ void pin2_tree(const BatchView &bv, int net, float c, int64_t *__restrict__ mst,
+                                          float *__restrict__ dist) {
+    if (!mst || bv.npin[net] != 2) return;
+    const int64_t o = bv.node_ofs[net];
+    mst[o] = ((int64_t)net << 30) | 1;
+    mst[o + 1] = -1;
+    if (dist) dist[net] = c;
+}
+
 __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                     Coords cd, const float *__restrict__ fen,
                                                     const float2 *__restrict__ tab,
-                                                    float *__restrict__ cost, int16_t *__restrict__ pat) {
+                                                    float *__restrict__ cost, int16_t *__restrict__ pat,
+                                                    int64_t *__restrict__ mst, float *__restrict__ dist) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
          p += (int64_t)gridDim.x * blockDim.x) {
         int net = ofs_search(bv.pair_ofs, bv.n, p);
@@ -230,6 +249,7 @@ __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const
         }
         cost[p] = c;
         pat[p] = (int16_t)cp;
+        pin2_tree(bv, net, c, mst, dist);
     }
 }
 
@@ -657,7 +677,8 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, 
 template <int ZC>
 __global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
-                                                float *__restrict__ cost, int16_t *__restrict__ pat) {
+                                                float *__restrict__ cost, int16_t *__restrict__ pat,
+                                                int64_t *__restrict__ mst, float *__restrict__ dist) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
          p += (int64_t)gridDim.x * blockDim.x) {
         const int net = ofs_search(bv.pair_ofs, bv.n, p);
@@ -680,6 +701,7 @@ __global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int
         }
         cost[p] = c;
         pat[p] = (int16_t)cp;
+        pin2_tree(bv, net, c, mst, dist);
     }
 }
 
@@ -858,44 +880,6 @@ __device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, cons
     return 1;
 }
 
-// Marks with one atomicOr per bitmap word. The bits a slot sets first are
-// the cells it owns for this batch; the slot lists them as (word, newly set
-// bits) entries. A summary bitmap holds one bit per mark word that has any
-// mark, so range scans skip empty 1024-cell blocks.
-constexpr int kEntBuf = 24;
-
-struct MarkVis {
-    uint32_t *mark;
-    uint32_t *sum;
-    unsigned long long *list;
-    int32_t *count;
-    unsigned long long ent[kEntBuf];
-    int n = 0;
-    __device__ __forceinline__ void add(int32_t w, uint32_t bits) {
-        const unsigned long long v = ((unsigned long long)(uint32_t)w << 32) | bits;
-        if (n < kEntBuf) ent[n++] = v;
-        else list[atomicAdd(count, 1)] = v;  // long paths: the rare overflow goes out one by one
-    }
-    __device__ __forceinline__ void word(int w, uint32_t m) {
-        const uint32_t old = atomicOr(mark + w, m);
-        const uint32_t nb = m & ~old;
-        if (nb) {
-            if (!old) atomicOr(sum + (w >> 5), 1u << (w & 31));
-            add(w, nb);
-        }
-    }
-    __device__ __forceinline__ void span(int32_t e0, int cnt) {
-        const int32_t e1 = e0 + cnt - 1;
-        for (int w = e0 >> 5; w <= (e1 >> 5); w++) {
-            uint32_t m = 0xffffffffu;
-            if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
-            if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
-            word(w, m);
-        }
-    }
-    __device__ __forceinline__ void cell(int32_t e) { word(e >> 5, 1u << (e & 31)); }
-};
-
 // The marking units of one edge's path: each via cell, and each 32-cell mark
 // word a wire covers (with the word's bits inside the wire).
 // A path has at most three layer changes of up to Z-2 interior cells and two
@@ -939,14 +923,31 @@ struct PathUnits {
     }
 };
 
-// One warp per MST slot: lane 0 lays out the edge's path units, the lanes
-// set their units' marks in parallel, and the (word, newly set bits) entries
-// are appended contiguously with one atomic per edge.
-__global__ void __launch_bounds__(256) k_mark6(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+
+// ---------------------------------------------------------------- commit by track
+// Routing tracks (a row of an even layer, a column of an odd layer) are
+// numbered layer by layer: layer z starts at track_first(z).
+__device__ __forceinline__ int track_first(const GridC &g, int z) { return ((z + 1) >> 1) * g.Y + (z >> 1) * g.X; }
+
+// track index and first cell of the track holding cell e
+__device__ __forceinline__ void track_of(const GridC &g, int32_t e, int &t, int32_t &base) {
+    const int z = e / g.XY;
+    const int r = e - z * g.XY;
+    const int L = (z & 1) ? g.Y : g.X;
+    const int row = r / L;
+    t = track_first(g, z) + row;
+    base = z * g.XY + row * L;
+}
+
+// One warp per MST slot, as k_mark6, but what the batch records is the set
+// of tracks that gained marked cells: each path unit (a via cell, or the
+// part of a wire inside one 32-cell mark word) lies in a single track, and
+// the first unit to set bits of a track flags it in a track bitmap and
+// appends the track's first cell to the track list.
+__global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                               int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *sum,
-                                               unsigned long long *__restrict__ list, int32_t *count,
-                                               uint32_t *status) {
+                                               int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *tbits,
+                                               int32_t *__restrict__ tlist, int32_t *tcount, uint32_t *status) {
     __shared__ PathUnits su[8];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -970,240 +971,130 @@ __global__ void __launch_bounds__(256) k_mark6(GridC g, BatchView bv, const int3
         }
         units = __shfl_sync(FULL, units, 0);
         __syncwarp();
-        int base = 0;
         for (int u0 = 0; u0 < units; u0 += 32) {
             const int u = u0 + lane;
-            int w = 0;
-            uint32_t nb = 0;
+            int32_t tb = 0;
+            bool fresh = false;
             if (u < units) {
+                int w;
                 uint32_t m;
                 pu.unit(u, w, m);
                 const uint32_t old = atomicOr(mark + w, m);
-                nb = m & ~old;
-                if (nb && !old) atomicOr(sum + (w >> 5), 1u << (w & 31));
+                if (m & ~old) {
+                    int t;
+                    track_of(g, (w << 5) + __ffs(m) - 1, t, tb);
+                    const uint32_t bit = 1u << (t & 31);
+                    fresh = !(atomicOr(tbits + (t >> 5), bit) & bit);
+                }
             }
-            const unsigned want = __ballot_sync(FULL, nb != 0);
+            const unsigned want = __ballot_sync(FULL, fresh);
             if (want) {
-                if (lane == 0) base = atomicAdd(count, __popc(want));
+                int base = 0;
+                if (lane == 0) base = atomicAdd(tcount, __popc(want));
                 base = __shfl_sync(FULL, base, 0);
-                if (nb)
-                    list[base + __popc(want & ((1u << lane) - 1))] = ((unsigned long long)(uint32_t)w << 32) | nb;
+                if (fresh) tlist[base + __popc(want & ((1u << lane) - 1))] = tb;
             }
         }
         __syncwarp();
     }
 }
 
-// Visits the marked cells of [lo, hi] in ascending order; f(cell) returns
-// false to stop. Reads one summary word per 1024 cells and only the non-empty
-// mark words.
-template <class F>
-__device__ __forceinline__ void scan_marks(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
-                                           int32_t lo, int32_t hi, F &&f) {
-    if (lo > hi) return;
-    const int wlo = lo >> 5, whi = hi >> 5;
-    for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
-        uint32_t sm = __ldg(sum + sw);
-        if (sw == (wlo >> 5)) sm &= 0xffffffffu << (wlo & 31);
-        if (sw == (whi >> 5)) sm &= 0xffffffffu >> (31 - (whi & 31));
-        while (sm) {
-            const int w = (sw << 5) + __ffs(sm) - 1;
-            sm &= sm - 1;
-            uint32_t m = __ldg(mark + w);
-            if (w == wlo) m &= 0xffffffffu << (lo & 31);
-            if (w == whi) m &= 0xffffffffu >> (31 - (hi & 31));
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                if (!f((w << 5) + b)) return;
-            }
-        }
-    }
-}
-
-// v += cost(cap-1) - cost(cap) of every marked q in [lo, hi], ascending
-// (bit_util.hpp:87-89 with the adds serialised in cell order). Each
-// non-empty mark word's 32 capacities come in as eight 16-byte loads issued
-// together; the marked cells' increments are then added in cell order.
-__device__ __forceinline__ float dlut_at(const float *dlut, int c) {
-    c = c < kLutMin ? kLutMin : (c > kLutMax + 1 ? kLutMax + 1 : c);
-    return dlut[c - kLutMin];
-}
-
-__device__ __forceinline__ void sum_marked(const uint32_t *__restrict__ mark, const uint32_t *__restrict__ sum,
-                                           const int32_t *__restrict__ capr, const float *dlut, int32_t lo,
-                                           int32_t hi, float &v) {
-    if (lo > hi) return;
-    const int wlo = lo >> 5, whi = hi >> 5;
-    for (int sw = wlo >> 5; sw <= (whi >> 5); sw++) {
-        uint32_t sm = __ldg(sum + sw);
-        if (sw == (wlo >> 5)) sm &= 0xffffffffu << (wlo & 31);
-        if (sw == (whi >> 5)) sm &= 0xffffffffu >> (31 - (whi & 31));
-        while (sm) {
-            const int w = (sw << 5) + __ffs(sm) - 1;
-            sm &= sm - 1;
-            uint32_t m = __ldg(mark + w);
-            if (w == wlo) m &= 0xffffffffu << (lo & 31);
-            if (w == whi) m &= 0xffffffffu >> (31 - (hi & 31));
-            if (!m) continue;
-            const int4 *q4 = reinterpret_cast<const int4 *>(capr + ((int64_t)w << 5));
-            int4 c4[8];
-#pragma unroll
-            for (int i = 0; i < 8; i++) c4[i] = __ldg(q4 + i);
-            const int *cc = reinterpret_cast<const int *>(c4);
-            float inc[32];
-#pragma unroll
-            for (int b = 0; b < 32; b++) inc[b] = ((m >> b) & 1u) ? dlut_at(dlut, cc[b]) : 0.0f;
-#pragma unroll
-            for (int b = 0; b < 32; b++)
-                if ((m >> b) & 1u) v += inc[b];
-        }
-    }
-}
-
-// For a marked cell at track position p: walk its update path
-// (bit_util.hpp:39-55). The cell owns node i while no other marked cell lies
-// in (p, i-1]; the owner adds the increments of every marked cell of the
-// node's range (i - lowbit(i), i] in ascending cell order. Each node touched
-// by the batch thus has exactly one writer and a fixed summation order.
-__device__ __forceinline__ void fen_owner_update(const GridC &g, int32_t e, const uint32_t *__restrict__ mark,
-                                                 const uint32_t *__restrict__ sum, const int32_t *__restrict__ capr,
-                                                 const float *dlut, float *__restrict__ fen) {
-    const int z = e / g.XY;
-    const int r = e - z * g.XY;
-    const int p = (z & 1) ? r % g.Y : r % g.X;
-    const int L = (z & 1) ? g.Y : g.X;
-    const int32_t base = e - p;
-    int32_t checked = e;  // no other marked cell in (e, checked]
-    for (int i = p + 1; i <= L; i += i & -i) {
-        const int32_t top = base + i - 1;
-        bool other = false;
-        scan_marks(mark, sum, checked + 1, top, [&](int32_t) {
-            other = true;
-            return false;
-        });
-        if (other) break;
-        checked = top;
-        float v = fen[top];
-        sum_marked(mark, sum, capr, dlut, base + i - (i & -i), top, v);
-        fen[top] = v;
-    }
-}
-
-// One thread per (marked cell, level of its update path). Level l of the
-// path of position p is node i_l (i_0 = p+1, i_{l+1} = i_l + lowbit(i_l));
-// the cell owns it when no other marked cell lies in (p, i_l - 1] -- a test
-// that needs no lower level, so all levels proceed in parallel. Level 0 is
-// always owned; levels >= 1 can only be owned when cell p+1 is unmarked, so
-// only such "span ends" get them. A warp takes up to 32 list entries (fewer
-// when the list is short) and deals out their (cell, level) items.
-__global__ void __launch_bounds__(256) k_fen_update8(GridC g, const unsigned long long *__restrict__ list,
-                                                     const int32_t *__restrict__ count,
-                                                     const uint32_t *__restrict__ mark,
-                                                     const uint32_t *__restrict__ sum,
-                                                     const int32_t *__restrict__ capr, const float *__restrict__ lut,
-                                                     float *__restrict__ fen, int levels) {
-    __shared__ int sx[8][32];
-    __shared__ uint32_t sw[8][32], sb[8][32], sends[8][32];
-    __shared__ float dlut[kLutMax - kLutMin + 2];  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
-    for (int c = threadIdx.x; c < kLutMax - kLutMin + 2; c += blockDim.x) dlut[c] = lut_inc(lut, c + kLutMin);
-    __syncthreads();
-    const int cnt = *count;
+// One warp per listed track (bit_util.hpp:75-90 for the cells the batch
+// marked on it): (1) the marked positions of the track and their increments
+// cost(cap-1) - cost(cap) are compacted in ascending order (shared memory
+// when the track fits, else the track's slice of a CSIZE scratch), each
+// cell's capacity drops by one and its mark bit is cleared; (2) every marked
+// cell walks its update path and, for each node where it is the highest
+// marked cell of the node's range (i - lowbit(i), i], adds the increments of
+// that range's marked cells to the node in ascending order -- the node's
+// updates in cell order, as a sequential commit makes them. Nodes thus have
+// one writer each; the track's cells are touched by this warp alone.
+__global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__restrict__ tlist,
+                                                      const int32_t *__restrict__ tcount, uint32_t *mark,
+                                                      uint32_t *tbits, int32_t *__restrict__ capr,
+                                                      const float *__restrict__ dlut, float *__restrict__ fen,
+                                                      int32_t *__restrict__ gpos, float *__restrict__ gdel,
+                                                      int cap) {
+    extern __shared__ int32_t tsm[];  // per warp: cap positions, then cap increments
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    int epw = cnt / warps;  // entries per warp
-    epw = epw < 1 ? 1 : (epw > 32 ? 32 : epw);
-    const int up = levels > 1 ? levels - 1 : 0;  // tracks of one cell have no higher levels
-    for (int e0 = (blockIdx.x * (blockDim.x >> 5) + wib) * epw; e0 < cnt; e0 += warps * epw) {
-        const int ei = e0 + lane;
-        int c = 0;
-        uint32_t w = 0, bits = 0, ends = 0;
-        if (lane < epw && ei < cnt) {
-            const unsigned long long it = list[ei];
-            w = (uint32_t)(it >> 32);
-            bits = (uint32_t)it;
-            const uint32_t mw = __ldg(mark + w), nx = __ldg(mark + w + 1);
-            ends = bits & ~((mw >> 1) | (nx << 31));  // next cell unmarked
-            c = __popc(bits) + __popc(ends) * up;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int cnt = *tcount;
+    int32_t *spos = tsm + (size_t)wib * 2 * cap;
+    float *sdel = reinterpret_cast<float *>(spos + cap);
+    for (int t = blockIdx.x * wpb + wib; t < cnt; t += gridDim.x * wpb) {
+        const int32_t base = tlist[t];
+        const int z = base / g.XY;
+        const int L = (z & 1) ? g.Y : g.X;
+        const int w0 = base >> 5, w1 = (base + L - 1) >> 5;
+        // marked count of the track
+        int total = 0;
+        for (int w = w0 + lane; w <= w1; w += 32) {
+            uint32_t m = mark[w];
+            if (w == w0) m &= 0xffffffffu << (base & 31);
+            if (w == w1) m &= 0xffffffffu >> (31 - ((base + L - 1) & 31));
+            total += __popc(m);
         }
-        int incl = c;
+        total = __reduce_add_sync(FULL, total);
+        int32_t *P = total <= cap ? spos : gpos + base;
+        float *D = total <= cap ? sdel : gdel + base;
+        // (1) compaction in position order
+        int run = 0;
+        for (int c0 = w0; c0 <= w1; c0 += 32) {
+            const int w = c0 + lane;
+            uint32_t m = 0;
+            if (w <= w1) {
+                m = mark[w];
+                if (w == w0) m &= 0xffffffffu << (base & 31);
+                if (w == w1) m &= 0xffffffffu >> (31 - ((base + L - 1) & 31));
+            }
+            const int pc = __popc(m);
+            int incl = pc;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int total = __shfl_sync(FULL, incl, 31);
-        sx[wib][lane] = incl - c;
-        sw[wib][lane] = w;
-        sb[wib][lane] = bits;
-        sends[wib][lane] = ends;
-        __syncwarp();
-        const int last = (epw < 32 ? epw : 32) - 1;
-        for (int t = lane; t < total; t += 32) {
-            int lo = 0, hi = last;  // last entry whose exclusive prefix is <= t
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sx[wib][mid] <= t) lo = mid;
-                else hi = mid - 1;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
             }
-            int k = t - sx[wib][lo];
-            const uint32_t bb = sb[wib][lo];
-            const int nb = __popc(bb);
-            uint32_t m;
-            int lv;
-            if (k < nb) {
-                m = bb;
-                lv = 0;
-            } else {  // only reached when up > 0
-                k -= nb;
-                m = sends[wib][lo];
-                lv = 1 + k % up;
-                k /= up;
+            int k = run + incl - pc;
+            run += __shfl_sync(FULL, incl, 31);
+            if (m) {
+                uint32_t b = m;
+                while (b) {
+                    const int e = (w << 5) + __ffs(b) - 1;
+                    b &= b - 1;
+                    const int cv = capr[e];
+                    P[k] = e - base;
+                    D[k] = __ldg(dlut + (cv < kLutMin ? 0 : (cv > kLutMax + 1 ? kLutMax + 1 - kLutMin : cv - kLutMin)));
+                    capr[e] = cv - 1;
+                    k++;
+                }
+                atomicAnd(mark + w, ~m);
             }
-            for (; k > 0; k--) m &= m - 1;  // drop the lower set bits
-            const int32_t e = ((int32_t)sw[wib][lo] << 5) + __ffs(m) - 1;
-            const int z = e / g.XY;
-            const int r = e - z * g.XY;
-            const int p = (z & 1) ? r % g.Y : r % g.X;
-            const int L = (z & 1) ? g.Y : g.X;
-            int i = p + 1;
-            for (int q = 0; q < lv; q++) i += i & -i;
-            if (i > L) continue;
-            const int32_t base = e - p, top = base + i - 1;
-            if (lv) {
-                bool other = false;
-                scan_marks(mark, sum, e + 1, top, [&](int32_t) {
-                    other = true;
-                    return false;
-                });
-                if (other) continue;
-            }
-            float v = fen[top];
-            sum_marked(mark, sum, capr, dlut, base + i - (i & -i), top, v);
-            fen[top] = v;
         }
         __syncwarp();
-    }
-}
-
-// demand += 1 for every marked cell (bit_util.hpp:88); marks and emptied
-// summary bits cleared for the next batch
-__global__ void k_finalize5(const unsigned long long *__restrict__ list, const int32_t *__restrict__ count,
-                            uint32_t *__restrict__ mark, uint32_t *__restrict__ sum, int32_t *__restrict__ capr) {
-    const int cnt = *count;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
-        const unsigned long long it = list[t];
-        const int32_t w = (int32_t)(it >> 32);
-        const uint32_t bits0 = (uint32_t)it;
-        uint32_t bits = bits0;
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            capr[(w << 5) + b] -= 1;
+        // (2) node updates, one owner per node
+        for (int k = lane; k < total; k += 32) {
+            const int p = P[k];
+            const int nxt = k + 1 < total ? P[k + 1] : L;  // next marked position (L: none)
+            for (int i = p + 1; i <= L && nxt >= i; i += i & -i) {
+                const int lo = i - (i & -i);  // range [lo, i-1], 0-based
+                int a = 0, b = k;             // first index with P >= lo
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    if (P[mid] < lo) a = mid + 1;
+                    else b = mid;
+                }
+                float v = fen[base + i - 1];
+                for (int j = a; j <= k; j++) v += D[j];
+                fen[base + i - 1] = v;
+            }
         }
-        const uint32_t old = atomicAnd(mark + w, ~bits0);
-        if ((old & ~bits0) == 0) atomicAnd(sum + (w >> 5), ~(1u << (w & 31)));
+        __syncwarp();
+        if (lane == 0) {
+            int tt;
+            int32_t bb;
+            track_of(g, base, tt, bb);
+            atomicAnd(tbits + (tt >> 5), ~(1u << (tt & 31)));
+        }
     }
 }
 

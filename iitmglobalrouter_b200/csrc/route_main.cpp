@@ -11,8 +11,7 @@
 // plus:
 //   -device d                    CUDA device (default 0)
 //   -report F                    JSON report: timings, nets/s, overflow, WL, vias
-// (Graph replay pays off for repeated routes of one plan -- gr_route_plan with
-// GR_PLAN_GRAPH -- not for this one-shot run; -graph is accepted and ignored.)
+//   -graph                       route the plan as one captured CUDA graph
 // Unknown flags are ignored (as the reference does). -rbt_part, -ord_part,
 // -upd_ispd24_net_file and running without -bit_pmodel select reference modes
 // this tool does not provide; it stops with a message.
@@ -125,7 +124,7 @@ int main(int argc, char **argv) {
     if ((rc = gr_sync(ctx))) return fail("setup", rc);
     const double t3 = now();
     rc = gr_route_design_host(ctx, n_nets, pin_ofs.data(), pins.data(), n_batches, bofs.data(), ids.data(),
-                              mst.data(), pat.data(), 0);
+                              mst.data(), pat.data(), a.graph ? GR_PLAN_GRAPH : 0);
     if (rc) return fail("routing", rc);
     const double t4 = now();
 

@@ -145,7 +145,8 @@ int gr_route_plan(gr_ctx *ctx, int32_t b0, int32_t b1, int64_t *d_mst_edges, int
                   void *stream);
 
 /* End to end with host buffers: upload nets and plan, reset, route every
- * batch, copy MST slots and patterns back (h_* are host pointers). */
+ * batch, copy MST slots and patterns back (h_* are host pointers).
+ * flags: GR_PLAN_GRAPH routes the plan as one captured CUDA graph. */
 int gr_route_design_host(gr_ctx *ctx, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins,
                          int32_t n_batches, const int64_t *h_batch_ofs, const int32_t *h_net_ids,
                          int64_t *h_mst_edges, int32_t *h_mst_pat, int flags);

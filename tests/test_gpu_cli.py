@@ -10,7 +10,7 @@ import iitmglobalrouter_b200 as gr
 import oracle
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("flags", [["-wrt_mrg", "-rseg_fmt", "-oprd_ppatch"], []])
+@pytest.mark.parametrize("flags", [["-wrt_mrg", "-rseg_fmt", "-oprd_ppatch"], [], ["-wrt_mrg", "-graph"]])
 def test_route_cli_matches_oracle(cuda, tmp_path, flags):
     d = gr.Design.generate(1, seed=4)
     cap, net, out = tmp_path / "d.cap", tmp_path / "d.net", tmp_path / "d.route"
