@@ -58,6 +58,25 @@ def net_bytes(d, ofs, pins, total_demand):
     return int(4 * Z * (w.astype(np.int64) * h).sum() + 4 * n.sum() + 12 * (n - 1).sum() + 16 * int(total_demand))
 
 
+def kernel_units(ofs, ids, committed):
+    """Algorithmic units and bytes of one route step per profiled kernel kind:
+    k_lpat reads two pins and writes a cost and a pattern per pair (14 B);
+    k_mark reads a slot and its pair's pattern and writes the slot's pattern
+    (14 B); Boruvka reads the net's pair costs and writes its slots and cost
+    sum (4 P + 8 n + 4 B); k_track_commit moves 16 B per committed GCELL
+    (capacity and Fenwick leaf, each read and written)."""
+    n = np.diff(ofs)[ids].astype(np.int64)
+    P = n * (n - 1) // 2
+    big, mid = n > 32, (n > 2) & (n <= 32)
+    return {
+        "k_lpat": (int(P.sum()), 14 * int(P.sum())),
+        "k_mark": (int(n.sum()), 14 * int(n.sum())),
+        "k_mst_large": (int(P[big].sum()), int((4 * P + 8 * n + 4)[big].sum())),
+        "k_mst_warp": (int(P[mid].sum()), int((4 * P + 8 * n + 4)[mid].sum())),
+        "k_track_commit": (int(committed), 16 * int(committed)),
+    }
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -277,17 +296,24 @@ def main():
     kern_total = sum(v[0] for v in kern.values())
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / kern_total, 4)}
                for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}
-    dominant = next(iter(kernels))
-
-    # roofline of the step (all kernels): algorithmic bytes per step / step time
-    bnet = net_bytes(d, ofs, pins, int(demand.sum()))
+    # roofline of the dominant kernel: its algorithmic bytes per launch over
+    # its average launch time in the profiled step; DRAM traffic per launch
+    # from the ncu per-unit figures, scaled by the units one launch processes
+    units = kernel_units(ofs, ids, int(demand.sum()))
+    dominant = next(k for k in kernels if k in units)
     peak, peak_kind = peaks()
-    achieved = bnet / (ms_step / 1e3) / 1e9
+    kd = kernels[dominant]
+    alg_per_launch = units[dominant][1] / kd["launches"]
+    achieved = alg_per_launch / (kd["ms"] / kd["launches"] / 1e3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "dram_traffic.json"
     if tf.exists():
-        tj = json.loads(tf.read_text())
-        traffic = tj.get("bytes_per_step")
+        pu = json.loads(tf.read_text()).get("per_unit", {}).get(dominant)
+        if pu:
+            traffic = pu["bytes"] * units[dominant][0] / kd["launches"]
+    # and of the whole step (all kernels, B_net summed over the nets)
+    bnet = net_bytes(d, ofs, pins, int(demand.sum()))
+    step_achieved = bnet / (ms_step / 1e3) / 1e9
 
     # end to end through the host-buffer C ABI call (pinned host memory)
     def pinned(a):
@@ -306,7 +332,7 @@ def main():
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_times.append(t1 - t0)
-    e2e_t = replicas.max_over_ranks(sum(e2e_times) / len(e2e_times), dist, dev)
+    e2e_t = replicas.max_over_ranks(statistics.median(e2e_times), dist, dev)
     assert np.array_equal(h_mst.numpy(), mst_h), "end-to-end result differs from the resident run"
     h2d = pins.nbytes + (ids.size * 36 + 64)  # design pins + plan descriptor (pin offsets stay on the host)
     d2h = M * 8 + M * 4
@@ -332,8 +358,9 @@ def main():
                    "batches": len(bofs) - 1, "seed": args.seed, "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MB write) before every timed step", "graph": True, "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": "route step (all kernels)",
-                     "algorithmic_bytes_per_step": bnet, "dominant_kernel": dominant},
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": dominant,
+                     "algorithmic_bytes_per_launch": alg_per_launch,
+                     "step": {"achieved": step_achieved, "frac": step_achieved / peak, "algorithmic_bytes": bnet}},
         "kernels": kernels,
         "cpu_baseline": cpu,
         "e2e": {"value": replicas.whole_job_rate(n_nets, e2e_t, world), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
