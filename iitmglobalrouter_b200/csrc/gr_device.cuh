@@ -96,6 +96,37 @@ __device__ __forceinline__ int ofs_search(const int64_t *__restrict__ ofs, int n
     return lo;
 }
 
+// The same search done by a whole warp for a warp-uniform t: each round the
+// 32 lanes probe 32 evenly spaced entries and the ballot of "<= t" narrows
+// the range 32-fold, so ceil(log32 n) rounds of one load per lane.
+__device__ __forceinline__ int warp_ofs_search(const int64_t *__restrict__ ofs, int n, int64_t t, int lane) {
+    int lo = 0, hi = n;  // invariant: ofs[lo] <= t, answer in [lo, hi)
+    while (hi - lo > 1) {
+        const int step = (hi - lo + 31) >> 5;
+        const int idx = lo + (lane + 1) * step;
+        const unsigned le = __ballot_sync(0xffffffffu, idx < hi && __ldg(ofs + idx) <= t);
+        lo += __popc(le) * step;  // probes at or below t form a prefix of the lanes
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
+// For lane-varying t >= t0 where i0 answers t0: the answer within the 32
+// entries from i0 (one load per lane, then a binary search over the lanes'
+// values), or a full search when t lies beyond them. All lanes take part.
+__device__ __forceinline__ int warp_ofs_window(const int64_t *__restrict__ ofs, int n, int i0, int64_t t, int lane) {
+    const int64_t o = i0 + lane < n ? __ldg(ofs + i0 + lane) : INT64_MAX;
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step; step >>= 1) {
+        const int64_t v = __shfl_sync(0xffffffffu, o, lo + step);
+        if (v <= t) lo += step;
+    }
+    const int i = i0 + lo;
+    if (lo == 31 && i + 1 < n && __ldg(ofs + i + 1) <= t) return ofs_search(ofs, n, t);
+    return i;
+}
+
 // ---------------------------------------------------------------------------
 // L-pattern evaluation (bit_util.hpp:134-191), generic over how prefix
 // queries are answered. Ev provides:

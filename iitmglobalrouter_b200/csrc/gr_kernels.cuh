@@ -176,9 +176,13 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
 // Entry (z, a, b) of a net's table: the two prefix queries at (x_a, y_b) on
 // layer z along the layer's direction (x on even layers, y on odd ones).
 __global__ void k_qtable(GridC g, BatchView bv, Coords cd, const float *__restrict__ fen, float2 *__restrict__ tab) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < bv.n_tab;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int net = ofs_search(bv.tab_ofs, bv.n, t);
+    const int lane = threadIdx.x & 31;
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); t0 < bv.n_tab;
+         t0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = t0 + lane;
+        const int net = warp_ofs_window(bv.tab_ofs, bv.n, warp_ofs_search(bv.tab_ofs, bv.n, t0, lane),
+                                        t < bv.n_tab ? t : bv.n_tab - 1, lane);
+        if (t >= bv.n_tab) continue;
         const int64_t local = t - bv.tab_ofs[net];
         const int nxy = bv.nxy[net], nx = nxy >> 16, ny = nxy & 0xffff;
         const int per = nx * ny;
@@ -213,9 +217,13 @@ __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const
                                                     const float2 *__restrict__ tab,
                                                     float *__restrict__ cost, int16_t *__restrict__ pat,
                                                     int64_t *__restrict__ mst, float *__restrict__ dist) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
-         p += (int64_t)gridDim.x * blockDim.x) {
-        int net = ofs_search(bv.pair_ofs, bv.n, p);
+    const int lane = threadIdx.x & 31;
+    for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
+         p0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = p0 + lane;
+        const int net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
+                                        p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
+        if (p >= bv.n_pairs) continue;
         int j, k;
         pair_decode(p - bv.pair_ofs[net], j, k);
         const int32_t *np = pins + bv.pin_base[net];
@@ -675,13 +683,17 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, 
 }
 
 template <int ZC>
-__global__ void __launch_bounds__(256) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
+__global__ void __launch_bounds__(256, 2) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
                                                 float *__restrict__ cost, int16_t *__restrict__ pat,
                                                 int64_t *__restrict__ mst, float *__restrict__ dist) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < bv.n_pairs;
-         p += (int64_t)gridDim.x * blockDim.x) {
-        const int net = ofs_search(bv.pair_ofs, bv.n, p);
+    const int lane = threadIdx.x & 31;
+    for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
+         p0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = p0 + lane;
+        const int net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
+                                        p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
+        if (p >= bv.n_pairs) continue;
         int j, k;
         pair_decode(p - bv.pair_ofs[net], j, k);
         const int32_t *np = pins + bv.pin_base[net];
@@ -861,8 +873,8 @@ struct EdgeRef {
 };
 __device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, const int32_t *__restrict__ pins,
                                        const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                       int64_t s, EdgeRef &r) {
-    r.net = ofs_search(bv.node_ofs, bv.n, s);
+                                       int64_t s, int net, EdgeRef &r) {
+    r.net = net;
     const int64_t E = mst[s];
     if (E == -1) return 0;
     const int n = bv.npin[r.net];
@@ -955,11 +967,12 @@ __global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int3
     PathUnits &pu = su[wib];
     for (int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; s < bv.n_nodes; s += nwarps) {
         int units = 0;
+        const int net = warp_ofs_search(bv.node_ofs, bv.n, s, lane);
         if (lane == 0) {
             pu.seg_n = 0;
             pu.seg_u[0] = 0;
             EdgeRef r;
-            const int ok = edge_of(g, bv, pins, mst, ppat, s, r);
+            const int ok = edge_of(g, bv, pins, mst, ppat, s, net, r);
             if (ok <= 0) {
                 if (mst_pat) mst_pat[s] = -1;
                 if (ok < 0) atomicOr(status, 0x1u);
