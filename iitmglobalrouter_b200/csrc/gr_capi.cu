@@ -73,6 +73,9 @@ struct gr_ctx {
     std::vector<int32_t> h_nxy;                                    // per design net: (nx << 16) | ny
     // per-call batch descriptor (device) + pinned staging
     DevBuf desc, pcost, ppat, tab, dist;
+    DevBuf out_mst, out_pat;             // results of gr_route_design_host
+    cudaStream_t copy_stream = nullptr;  // its result copies, overlapping the route
+    cudaEvent_t ev_out = nullptr;
     void *h_stage = nullptr;
     size_t h_stage_bytes = 0;
     cudaEvent_t stage_done = nullptr;
@@ -561,6 +564,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GR_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
     for (int i = 0; i < 3; i++)
         if (cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
@@ -650,6 +656,10 @@ int gr_destroy(gr_ctx *c) {
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     if (c->stage_done) cudaEventDestroy(c->stage_done);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
+    if (c->ev_out) cudaEventDestroy(c->ev_out);
+    free_buf(c->out_mst);
+    free_buf(c->out_pat);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -677,14 +687,20 @@ int gr_reset(gr_ctx *c, void *stream) {
 
 int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins) {
     if (!c || n_nets < 0 || !h_pin_ofs || (n_nets > 0 && !h_pins) || h_pin_ofs[0] != 0) return GR_ERR_ARG;
+    int short_net = 0, long_net = 0, bad_pin = 0;
+#pragma omp parallel for reduction(| : short_net, long_net)
     for (int32_t i = 0; i < n_nets; i++) {
-        int64_t k = h_pin_ofs[i + 1] - h_pin_ofs[i];
-        if (k < 2) return GR_ERR_ARG;
-        if (k > GR_MAX_PINS) return GR_ERR_NET_TOO_LARGE;
+        const int64_t k = h_pin_ofs[i + 1] - h_pin_ofs[i];
+        short_net |= k < 2;
+        long_net |= k > GR_MAX_PINS;
     }
-    int64_t total = h_pin_ofs[n_nets];
-    for (int64_t t = 0; t < total; t++)
-        if (h_pins[t] < 0 || h_pins[t] >= c->csize) return GR_ERR_ARG;
+    if (short_net) return GR_ERR_ARG;
+    if (long_net) return GR_ERR_NET_TOO_LARGE;
+    const int64_t total = h_pin_ofs[n_nets];
+    const int64_t csize = c->csize;
+#pragma omp parallel for reduction(| : bad_pin)
+    for (int64_t t = 0; t < total; t++) bad_pin |= h_pins[t] < 0 || h_pins[t] >= csize;
+    if (bad_pin) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
     if ((size_t)(total + 1) > c->pins_cap) {
@@ -918,25 +934,48 @@ int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, co
     if ((rc = gr_set_nets(c, n_nets, h_pin_ofs, h_pins))) return rc;
     if ((rc = gr_plan_set(c, n_batches, h_batch_ofs, h_net_ids))) return rc;
     if ((rc = gr_reset(c, nullptr))) return rc;
-    int64_t slots = c->plan_slots;
-    DevBuf mst, pat;
-    if ((rc = ensure(mst, sizeof(int64_t) * (slots + 1), c->stream)) ||
-        (rc = ensure(pat, sizeof(int32_t) * (slots + 1), c->stream))) {
-        free_buf(mst);
-        free_buf(pat);
+    const int64_t slots = c->plan_slots;
+    if ((rc = ensure(c->out_mst, sizeof(int64_t) * (slots + 1), c->stream)) ||
+        (rc = ensure(c->out_pat, sizeof(int32_t) * (slots + 1), c->stream)))
         return rc;
+    int64_t *mst = (int64_t *)c->out_mst.p;
+    int32_t *pat = (int32_t *)c->out_pat.p;
+    // with page-locked results, each chunk of batches is copied back on the
+    // copy stream while the next chunks route
+    auto pinned = [](const void *h) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    };
+    const bool overlap = !(flags & GR_PLAN_GRAPH) && pinned(h_mst_edges) && (!h_mst_pat || pinned(h_mst_pat));
+    if (!overlap) {
+        rc = gr_route_plan(c, 0, n_batches, mst, pat, flags, nullptr);
+        if (!rc) {
+            GR_CK(cudaMemcpyAsync(h_mst_edges, mst, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream));
+            if (h_mst_pat)
+                GR_CK(cudaMemcpyAsync(h_mst_pat, pat, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream));
+        }
+    } else {
+        const int32_t chunk = 32;
+        for (int32_t b0 = 0; b0 < n_batches && !rc; b0 += chunk) {
+            const int32_t b1 = b0 + chunk < n_batches ? b0 + chunk : n_batches;
+            if ((rc = gr_route_plan(c, b0, b1, mst, pat, 0, nullptr))) break;
+            const int64_t s0 = c->plan[b0].slot0, s1 = b1 < n_batches ? c->plan[b1].slot0 : slots;
+            GR_CK(cudaEventRecord(c->ev_out, c->stream));
+            GR_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_out, 0));
+            GR_CK(cudaMemcpyAsync(h_mst_edges + s0, mst + s0, sizeof(int64_t) * (s1 - s0), cudaMemcpyDeviceToHost,
+                                  c->copy_stream));
+            if (h_mst_pat)
+                GR_CK(cudaMemcpyAsync(h_mst_pat + s0, pat + s0, sizeof(int32_t) * (s1 - s0),
+                                      cudaMemcpyDeviceToHost, c->copy_stream));
+        }
+        GR_CK(cudaStreamSynchronize(c->copy_stream));
     }
-    rc = gr_route_plan(c, 0, n_batches, (int64_t *)mst.p, (int32_t *)pat.p, flags, nullptr);
-    if (!rc) {
-        cudaMemcpyAsync(h_mst_edges, mst.p, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream);
-        if (h_mst_pat) cudaMemcpyAsync(h_mst_pat, pat.p, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream);
-        rc = gr_sync(c);
-    }
-    cudaStreamSynchronize(c->stream);
-    if (c->graph.mst == mst.p) drop_graph(c);  // the captured plan writes into the buffers freed here
-    free_buf(mst);
-    free_buf(pat);
-    return rc;
+    const int sr = gr_sync(c);
+    return rc ? rc : sr;
 }
 
 int gr_sync(gr_ctx *c) {
