@@ -75,6 +75,15 @@ SIGNATURES = {
     "gr_design_set_plan": (_I, [_P, C.c_int32, _P, _P]),
     "gr_design_write_routes": (_I, [_P, C.c_char_p, _P, _P, _I, _I, _P]),
     "gr_design_eval": (_I, [_P, _P, _P]),
+    "gr_cnn_create": (_I, [_PP, _I, _I, _I, _I, _I, _I, _I, _U64]),
+    "gr_cnn_destroy": (_I, [_P]),
+    "gr_cnn_num_params": (_I64, [_P]),
+    "gr_cnn_get_params": (_I, [_P, _P]),
+    "gr_cnn_set_params": (_I, [_P, _P]),
+    "gr_cnn_forward": (_I, [_P, _P, _P]),
+    "gr_cnn_grads": (_I, [_P, _P, _P, _P, _P]),
+    "gr_cnn_train_step": (_I, [_P, _P, _P, C.c_float, _P]),
+    "gr_cnn_gemm_test": (_I, [_I, _I, _I, _P, _P, _P, _I]),
 }
 
 _lib = None

@@ -30,7 +30,7 @@ CUDA_FLAGS = ARCH + [
 CXX = os.environ.get("GR_CXX", "g++")
 CXX_FLAGS = ["-O3", "-std=c++20", "-fPIC", "-fopenmp", "-I", str(ROOT / "include")]
 
-LIB_CU = ["gr_capi.cu"]
+LIB_CU = ["gr_capi.cu", "gr_cnn.cu"]
 LIB_CPP = ["gr_io.cpp", "gr_io_capi.cpp"]
 HEADERS = ["gr_device.cuh", "gr_kernels.cuh", "gr_io.hpp"]
 

@@ -1,0 +1,504 @@
+// gr_cnn.cu -- the congestion lookahead network: a stack of 3x3 convolutions
+// over the per-layer demand / capacity grid, BF16 tensor-core GEMMs with FP32
+// accumulation, trained and run entirely by the kernels in this file.
+//
+// A layer maps Cin channels of an H x W grid to Cout channels:
+//   forward   col[m][k] = X[ci][y+dy][x+dx]          (im2col, k = ci*9 + (dy+1)*3 + dx+1, m = y*W + x)
+//             Z[m][n]   = sum_k col[m][k] * Wt[k][n] (GEMM, mma.sync m16n8k16 bf16 -> f32)
+//             Y[n][m]   = act(Z[m][n] + b[n])         (ReLU on every layer but the last)
+//   backward  dZ = dY * act'(Z)
+//             dWt[k][n] = sum_m col[m][k] dZ[m][n]    (GEMM over the positions, split across blocks)
+//             db[n]     = sum_m dZ[m][n]
+//             dcol[m][k]= sum_n dZ[m][n] Wt[k][n]      (GEMM)
+//             dX        = col2im(dcol)                 (each input gathers its nine taps)
+// The loss is the mean squared error of the last layer against the target;
+// parameters are FP32 masters updated by Adam, cast to BF16 for the GEMMs.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/iitmgr_b200.h"
+
+namespace {
+
+#define CN_CK(call)                                                                                \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess) {                                                                   \
+            fprintf(stderr, "iitmgr_b200: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(_e), \
+                    __FILE__, __LINE__);                                                           \
+            return GR_ERR_CUDA;                                                                    \
+        }                                                                                          \
+    } while (0)
+
+constexpr int kMaxLayers = 8;
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// ------------------------------------------------------------------ GEMM
+// C[m][n] (f32) = or += sum over k in this block's range of A(m,k) * B(k,n),
+// A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn] (bf16), C(m,n) at
+// C[m*scm + n*scn]. Block tile 64 x 32, four warps of 16 rows each, k steps
+// of 16 staged in shared memory; out-of-range elements read as zero.
+// blockIdx.z splits the k range (atomic = 1 adds into C with atomics).
+constexpr int kBM = 64, kBN = 32, kBK = 16;
+
+__device__ __forceinline__ uint32_t pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bfloat16 *__restrict__ A,
+                                              long long sam, long long sak, const __nv_bfloat16 *__restrict__ B,
+                                              long long sbk, long long sbn, float *__restrict__ C, long long scm,
+                                              long long scn, int kchunk, int atomic) {
+    __shared__ __nv_bfloat16 As[kBM][kBK + 2];
+    __shared__ __nv_bfloat16 Bs[kBK][kBN + 2];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    float acc[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[j][q] = 0.0f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+    for (int k0 = kb; k0 < ke; k0 += kBK) {
+        for (int i = tid; i < kBM * kBK; i += 128) {
+            const int r = i / kBK, c = i % kBK, m = m0 + r, k = k0 + c;
+            As[r][c] = (m < M && k < ke) ? A[(long long)m * sam + (long long)k * sak] : zero;
+        }
+        for (int i = tid; i < kBK * kBN; i += 128) {
+            const int r = i / kBN, c = i % kBN, k = k0 + r, n = n0 + c;
+            Bs[r][c] = (k < ke && n < N) ? B[(long long)k * sbk + (long long)n * sbn] : zero;
+        }
+        __syncthreads();
+        const int r0 = warp * 16;
+        uint32_t a[4];
+        a[0] = pack2(As[r0 + g][2 * t], As[r0 + g][2 * t + 1]);
+        a[1] = pack2(As[r0 + g + 8][2 * t], As[r0 + g + 8][2 * t + 1]);
+        a[2] = pack2(As[r0 + g][2 * t + 8], As[r0 + g][2 * t + 9]);
+        a[3] = pack2(As[r0 + g + 8][2 * t + 8], As[r0 + g + 8][2 * t + 9]);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int nn = j * 8 + g;
+            const uint32_t b0 = pack2(Bs[2 * t][nn], Bs[2 * t + 1][nn]);
+            const uint32_t b1 = pack2(Bs[2 * t + 8][nn], Bs[2 * t + 9][nn]);
+            asm volatile(
+                "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                "{%0,%1,%2,%3};\n"
+                : "+f"(acc[j][0]), "+f"(acc[j][1]), "+f"(acc[j][2]), "+f"(acc[j][3])
+                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int m = m0 + warp * 16 + g + (q >= 2 ? 8 : 0), n = n0 + j * 8 + 2 * t + (q & 1);
+            if (m < M && n < N) {
+                float *p = C + (long long)m * scm + (long long)n * scn;
+                if (atomic) atomicAdd(p, acc[j][q]);
+                else *p = acc[j][q];
+            }
+        }
+}
+
+// ------------------------------------------------------------------ layer pieces
+__global__ void k_im2col(int Cin, int H, int W, int Kp, const float *__restrict__ X, __nv_bfloat16 *__restrict__ col) {
+    const long long total = (long long)H * W * Kp;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i % Kp);
+        const long long m = i / Kp;
+        const int y = (int)(m / W), x = (int)(m % W);
+        float v = 0.0f;
+        if (k < Cin * 9) {
+            const int ci = k / 9, r = k % 9, yy = y + r / 3 - 1, xx = x + r % 3 - 1;
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = X[((long long)ci * H + yy) * W + xx];
+        }
+        col[i] = __float2bfloat16(v);
+    }
+}
+
+// Y[n][m] = act(Z[m][n] + b[n]); keeps Z (pre-activation) for the backward pass
+__global__ void k_bias_act(int M, int Cout, int Np, const float *__restrict__ Z, const float *__restrict__ b,
+                           float *__restrict__ Y, int relu) {
+    const long long total = (long long)M * Cout;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int n = (int)(i / M);
+        const long long m = i % M;
+        const float v = Z[m * Np + n] + b[n];
+        Y[i] = relu ? fmaxf(v, 0.0f) : v;
+    }
+}
+
+// dZ[m][n] (bf16, padded to Np columns) = dY[n][m] * act'(Z + b)
+__global__ void k_act_grad(int M, int Cout, int Np, const float *__restrict__ dY, const float *__restrict__ Z,
+                           const float *__restrict__ b, __nv_bfloat16 *__restrict__ dZ, int relu) {
+    const long long total = (long long)M * Np;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int n = (int)(i % Np);
+        const long long m = i / Np;
+        float v = 0.0f;
+        if (n < Cout) {
+            v = dY[(long long)n * M + m];
+            if (relu && Z[m * Np + n] + b[n] <= 0.0f) v = 0.0f;
+        }
+        dZ[i] = __float2bfloat16(v);
+    }
+}
+
+// db[n] = sum_m dZ[m][n]: one block per output channel
+__global__ void k_bias_grad(int M, int Np, const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ db) {
+    __shared__ float red[256];
+    const int n = blockIdx.x;
+    float s = 0.0f;
+    for (long long m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(dZ[m * Np + n]);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) db[n] = red[0];
+}
+
+// dX[ci][y][x] = sum over taps of dcol[(y - dy) * W + (x - dx)][ci*9 + tap]
+__global__ void k_col2im(int Cin, int H, int W, int Kp, const float *__restrict__ dcol, float *__restrict__ dX) {
+    const long long total = (long long)Cin * H * W;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int ci = (int)(i / ((long long)H * W));
+        const int rem = (int)(i % ((long long)H * W));
+        const int y = rem / W, x = rem % W;
+        float s = 0.0f;
+        for (int r = 0; r < 9; r++) {
+            const int yy = y - (r / 3 - 1), xx = x - (r % 3 - 1);
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) s += dcol[((long long)yy * W + xx) * Kp + ci * 9 + r];
+        }
+        dX[i] = s;
+    }
+}
+
+// dY = 2 (Y - T) / count; partial sums of the squared error into loss[0]
+__global__ void k_mse(long long count, const float *__restrict__ Y, const float *__restrict__ T,
+                      float *__restrict__ dY, float *__restrict__ loss) {
+    __shared__ float red[256];
+    float s = 0.0f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float d = Y[i] - T[i];
+        dY[i] = 2.0f * d / (float)count;
+        s += d * d;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, red[0] / (float)count);
+}
+
+// weight layout conversions: W[co][ci][3][3] (f32 master) <-> Wt[k][n] (bf16 GEMM operand)
+__global__ void k_pack_w(int Cin, int Cout, int Kp, int Np, const float *__restrict__ Wm,
+                         __nv_bfloat16 *__restrict__ Wt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Kp * Np; i += gridDim.x * blockDim.x) {
+        const int k = i / Np, n = i % Np;
+        const float v = (k < Cin * 9 && n < Cout) ? Wm[n * Cin * 9 + k] : 0.0f;
+        Wt[i] = __float2bfloat16(v);
+    }
+}
+
+// g[co][ci*9 + r] = dWt[k][n]
+__global__ void k_unpack_grad(int Cin, int Cout, int Np, const float *__restrict__ dWt, float *__restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Cout * Cin * 9; i += gridDim.x * blockDim.x) {
+        const int n = i / (Cin * 9), k = i % (Cin * 9);
+        g[i] = dWt[k * Np + n];
+    }
+}
+
+__global__ void k_adam(int n, float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m1,
+                       float *__restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        m1[i] = b1 * m1[i] + (1.0f - b1) * gi;
+        m2[i] = b2 * m2[i] + (1.0f - b2) * gi * gi;
+        p[i] -= lr * (m1[i] / c1) / (sqrtf(m2[i] / c2) + eps);
+    }
+}
+
+int grid(long long items) {
+    long long b = (items + 255) / 256;
+    return (int)(b < 4096 ? (b > 0 ? b : 1) : 4096);
+}
+
+}  // namespace
+
+struct gr_cnn {
+    int device = 0, H = 0, W = 0, n_layers = 0;
+    int cin[kMaxLayers] = {}, cout[kMaxLayers] = {}, Kp[kMaxLayers] = {}, Np[kMaxLayers] = {};
+    int64_t w_ofs[kMaxLayers + 1] = {};  // parameter offsets: weights then bias, per layer
+    int64_t n_params = 0;
+    float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
+    __nv_bfloat16 *wt[kMaxLayers] = {};
+    float *dwt[kMaxLayers] = {};
+    float *act[kMaxLayers + 1] = {};  // act[0] = input, act[l+1] = output of layer l
+    float *z[kMaxLayers] = {};
+    __nv_bfloat16 *col = nullptr, *dz = nullptr;
+    float *dcol = nullptr, *dact = nullptr, *dact2 = nullptr, *loss = nullptr;
+    int64_t adam_t = 0;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+int gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16 *A, long long sam, long long sak,
+         const __nv_bfloat16 *B, long long sbk, long long sbn, float *C, long long scm, long long scn, int splits) {
+    int kchunk = round_up((K + splits - 1) / splits, kBK);
+    dim3 g((M + kBM - 1) / kBM, (N + kBN - 1) / kBN, (K + kchunk - 1) / kchunk);
+    k_gemm<<<g, 128, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, scm, scn, kchunk, g.z > 1 ? 1 : 0);
+    CN_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int pack_all(gr_cnn *c) {
+    for (int l = 0; l < c->n_layers; l++) {
+        k_pack_w<<<grid((long long)c->Kp[l] * c->Np[l]), 256, 0, c->stream>>>(c->cin[l], c->cout[l], c->Kp[l], c->Np[l],
+                                                                               c->params + c->w_ofs[l], c->wt[l]);
+    }
+    CN_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int forward(gr_cnn *c) {
+    const int M = c->H * c->W;
+    cudaStream_t s = c->stream;
+    for (int l = 0; l < c->n_layers; l++) {
+        k_im2col<<<grid((long long)M * c->Kp[l]), 256, 0, s>>>(c->cin[l], c->H, c->W, c->Kp[l], c->act[l], c->col);
+        int rc = gemm(s, M, c->Np[l], c->Kp[l], c->col, c->Kp[l], 1, c->wt[l], c->Np[l], 1, c->z[l], c->Np[l], 1, 1);
+        if (rc) return rc;
+        const float *b = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
+        k_bias_act<<<grid((long long)M * c->cout[l]), 256, 0, s>>>(M, c->cout[l], c->Np[l], c->z[l], b,
+                                                                   c->act[l + 1], l + 1 < c->n_layers);
+    }
+    CN_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+// gradients of the mean squared error against d_target into c->grads
+int backward(gr_cnn *c, const float *d_target) {
+    const int M = c->H * c->W, L = c->n_layers;
+    cudaStream_t s = c->stream;
+    const long long cnt = (long long)c->cout[L - 1] * M;
+    CN_CK(cudaMemsetAsync(c->loss, 0, sizeof(float), s));
+    k_mse<<<grid(cnt), 256, 0, s>>>(cnt, c->act[L], d_target, c->dact, c->loss);
+    float *dY = c->dact, *dX = c->dact2;
+    for (int l = L - 1; l >= 0; l--) {
+        const int relu = l + 1 < L, Kp = c->Kp[l], Np = c->Np[l], cin = c->cin[l], co = c->cout[l];
+        const float *b = c->params + c->w_ofs[l] + (int64_t)co * cin * 9;
+        k_act_grad<<<grid((long long)M * Np), 256, 0, s>>>(M, co, Np, dY, c->z[l], b, c->dz, relu);
+        // the layer's input again as columns (col holds the last layer's)
+        k_im2col<<<grid((long long)M * Kp), 256, 0, s>>>(cin, c->H, c->W, Kp, c->act[l], c->col);
+        CN_CK(cudaMemsetAsync(c->dwt[l], 0, sizeof(float) * Kp * Np, s));
+        int rc = gemm(s, Kp, Np, M, c->col, 1, Kp, c->dz, Np, 1, c->dwt[l], Np, 1, 64);
+        if (rc) return rc;
+        float *g = c->grads + c->w_ofs[l];
+        k_unpack_grad<<<grid((long long)co * cin * 9), 256, 0, s>>>(cin, co, Np, c->dwt[l], g);
+        k_bias_grad<<<co, 256, 0, s>>>(M, Np, c->dz, g + (int64_t)co * cin * 9);
+        if (l > 0) {
+            rc = gemm(s, M, Kp, Np, c->dz, Np, 1, c->wt[l], 1, Np, c->dcol, Kp, 1, 1);
+            if (rc) return rc;
+            k_col2im<<<grid((long long)cin * M), 256, 0, s>>>(cin, c->H, c->W, Kp, c->dcol, dX);
+            float *t = dY;
+            dY = dX;
+            dX = t;
+        }
+    }
+    CN_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, int hidden, int n_layers, int H,
+                  int W, uint64_t seed) {
+    if (!out || in_channels < 1 || out_channels < 1 || hidden < 1 || hidden > 32 || n_layers < 2 ||
+        n_layers > kMaxLayers || H < 1 || W < 1 || out_channels > 32)
+        return GR_ERR_ARG;
+    *out = nullptr;
+    CN_CK(cudaSetDevice(device));
+    gr_cnn *c = new gr_cnn();
+    c->device = device;
+    c->H = H;
+    c->W = W;
+    c->n_layers = n_layers;
+    int64_t ofs = 0, kmax = 0, nmax = 0, cmax = in_channels;
+    for (int l = 0; l < n_layers; l++) {
+        c->cin[l] = l == 0 ? in_channels : hidden;
+        c->cout[l] = l + 1 == n_layers ? out_channels : hidden;
+        c->Kp[l] = round_up(c->cin[l] * 9, 16);
+        c->Np[l] = round_up(c->cout[l], 8);
+        c->w_ofs[l] = ofs;
+        ofs += (int64_t)c->cout[l] * c->cin[l] * 9 + c->cout[l];
+        kmax = c->Kp[l] > kmax ? c->Kp[l] : kmax;
+        nmax = c->Np[l] > nmax ? c->Np[l] : nmax;
+        cmax = c->cout[l] > cmax ? c->cout[l] : cmax;
+    }
+    c->w_ofs[n_layers] = ofs;
+    c->n_params = ofs;
+    const int64_t M = (int64_t)H * W;
+    auto fail = [&](int code) {
+        gr_cnn_destroy(c);
+        return code;
+    };
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->params, sizeof(float) * ofs) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->grads, sizeof(float) * ofs) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->m1, sizeof(float) * ofs) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->m2, sizeof(float) * ofs) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->col, sizeof(__nv_bfloat16) * M * kmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->dz, sizeof(__nv_bfloat16) * M * nmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->dcol, sizeof(float) * M * kmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->dact, sizeof(float) * M * cmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->dact2, sizeof(float) * M * cmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->loss, sizeof(float) * 2) == cudaSuccess;
+    for (int l = 0; l <= n_layers && ok; l++)
+        ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
+    for (int l = 0; l < n_layers && ok; l++) {
+        ok = cudaMalloc(&c->wt[l], sizeof(__nv_bfloat16) * c->Kp[l] * c->Np[l]) == cudaSuccess &&
+             cudaMalloc(&c->z[l], sizeof(float) * M * c->Np[l]) == cudaSuccess &&
+             cudaMalloc(&c->dwt[l], sizeof(float) * c->Kp[l] * c->Np[l]) == cudaSuccess;
+    }
+    if (!ok) {
+        cudaGetLastError();
+        return fail(GR_ERR_NOMEM);
+    }
+    // He-uniform weights from a fixed-seed generator (splitmix64), zero biases
+    std::vector<float> h(ofs, 0.0f);
+    uint64_t st = seed ? seed : 1;
+    auto rnd = [&]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) / 9007199254740992.0;
+    };
+    for (int l = 0; l < n_layers; l++) {
+        const double a = std::sqrt(6.0 / (c->cin[l] * 9.0));
+        for (int64_t i = 0; i < (int64_t)c->cout[l] * c->cin[l] * 9; i++) h[c->w_ofs[l] + i] = (float)((2 * rnd() - 1) * a);
+    }
+    if (cudaMemcpy(c->params, h.data(), sizeof(float) * ofs, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(c->m1, 0, sizeof(float) * ofs) != cudaSuccess ||
+        cudaMemset(c->m2, 0, sizeof(float) * ofs) != cudaSuccess || pack_all(c) != GR_OK ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
+    *out = c;
+    return GR_OK;
+}
+
+int gr_cnn_destroy(gr_cnn *c) {
+    if (!c) return GR_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : {(void *)c->params, (void *)c->grads, (void *)c->m1, (void *)c->m2, (void *)c->col, (void *)c->dz,
+                    (void *)c->dcol, (void *)c->dact, (void *)c->dact2, (void *)c->loss})
+        cudaFree(p);
+    for (int l = 0; l < kMaxLayers; l++) {
+        cudaFree(c->wt[l]);
+        cudaFree(c->z[l]);
+        cudaFree(c->dwt[l]);
+    }
+    for (int l = 0; l <= kMaxLayers; l++) cudaFree(c->act[l]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GR_OK;
+}
+
+int64_t gr_cnn_num_params(gr_cnn *c) { return c ? c->n_params : -1; }
+
+int gr_cnn_get_params(gr_cnn *c, float *h_out) {
+    if (!c || !h_out) return GR_ERR_ARG;
+    CN_CK(cudaStreamSynchronize(c->stream));
+    CN_CK(cudaMemcpy(h_out, c->params, sizeof(float) * c->n_params, cudaMemcpyDeviceToHost));
+    return GR_OK;
+}
+
+int gr_cnn_set_params(gr_cnn *c, const float *h_in) {
+    if (!c || !h_in) return GR_ERR_ARG;
+    CN_CK(cudaStreamSynchronize(c->stream));
+    CN_CK(cudaMemcpy(c->params, h_in, sizeof(float) * c->n_params, cudaMemcpyHostToDevice));
+    int rc = pack_all(c);
+    if (rc) return rc;
+    CN_CK(cudaStreamSynchronize(c->stream));
+    return GR_OK;
+}
+
+int gr_cnn_forward(gr_cnn *c, const float *d_in, float *d_out) {
+    if (!c || !d_in || !d_out) return GR_ERR_ARG;
+    const int64_t M = (int64_t)c->H * c->W;
+    CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
+    int rc = forward(c);
+    if (rc) return rc;
+    CN_CK(cudaMemcpyAsync(d_out, c->act[c->n_layers], sizeof(float) * M * c->cout[c->n_layers - 1],
+                          cudaMemcpyDeviceToDevice, c->stream));
+    CN_CK(cudaStreamSynchronize(c->stream));
+    return GR_OK;
+}
+
+int gr_cnn_grads(gr_cnn *c, const float *d_in, const float *d_target, float *h_grads, float *h_loss) {
+    if (!c || !d_in || !d_target) return GR_ERR_ARG;
+    const int64_t M = (int64_t)c->H * c->W;
+    CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
+    int rc = forward(c);
+    if (!rc) rc = backward(c, d_target);
+    if (rc) return rc;
+    if (h_grads)
+        CN_CK(cudaMemcpyAsync(h_grads, c->grads, sizeof(float) * c->n_params, cudaMemcpyDeviceToHost, c->stream));
+    if (h_loss) CN_CK(cudaMemcpyAsync(h_loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CN_CK(cudaStreamSynchronize(c->stream));
+    return GR_OK;
+}
+
+int gr_cnn_train_step(gr_cnn *c, const float *d_in, const float *d_target, float lr, float *h_loss) {
+    if (!c || !d_in || !d_target || !(lr > 0.0f)) return GR_ERR_ARG;
+    const int64_t M = (int64_t)c->H * c->W;
+    CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
+    int rc = forward(c);
+    if (!rc) rc = backward(c, d_target);
+    if (rc) return rc;
+    c->adam_t++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - (float)std::pow((double)b1, (double)c->adam_t);
+    const float c2 = 1.0f - (float)std::pow((double)b2, (double)c->adam_t);
+    k_adam<<<grid(c->n_params), 256, 0, c->stream>>>((int)c->n_params, c->params, c->grads, c->m1, c->m2, lr, b1, b2,
+                                                      1e-8f, c1, c2);
+    CN_CK(cudaGetLastError());
+    rc = pack_all(c);
+    if (rc) return rc;
+    if (h_loss) CN_CK(cudaMemcpyAsync(h_loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CN_CK(cudaStreamSynchronize(c->stream));
+    return GR_OK;
+}
+
+// test hook: one GEMM C = A * B of row-major bf16 matrices (A: M x K, B: K x N),
+// C f32 row-major, with the k range split over `splits` blocks
+int gr_cnn_gemm_test(int M, int N, int K, const void *d_a, const void *d_b, float *d_c, int splits) {
+    if (M < 1 || N < 1 || K < 1 || !d_a || !d_b || !d_c || splits < 1) return GR_ERR_ARG;
+    CN_CK(cudaMemset(d_c, 0, sizeof(float) * M * N));
+    int rc = gemm(nullptr, M, N, K, (const __nv_bfloat16 *)d_a, K, 1, (const __nv_bfloat16 *)d_b, N, 1, d_c, N, 1,
+                  splits);
+    if (rc) return rc;
+    CN_CK(cudaDeviceSynchronize());
+    return GR_OK;
+}
+
+}  // extern "C"

@@ -237,6 +237,28 @@ int gr_design_write_routes(const gr_design *d, const char *path, const int64_t *
 /* out3 = {overflow, overflowed cells, total demand} for a demand grid */
 int gr_design_eval(const gr_design *d, const int32_t *demand, double *out3);
 
+/* ------------------------------------------------------------ congestion lookahead network
+ * No counterpart in the reference: a stack of n_layers 3x3 convolutions
+ * (hidden channels, ReLU between layers) mapping in_channels grids of H x W
+ * (channel-major f32, [c][y][x]) to out_channels grids -- per routing layer
+ * the demand still to come, predicted from the current demand and capacity.
+ * BF16 tensor-core GEMMs with FP32 accumulation, FP32 master parameters
+ * (per layer: weights [cout][cin][3][3], then biases), Adam updates on a
+ * mean-squared-error loss. d_* are device pointers; calls synchronise. */
+typedef struct gr_cnn gr_cnn;
+int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, int hidden, int n_layers, int H,
+                  int W, uint64_t seed);
+int gr_cnn_destroy(gr_cnn *cnn);
+int64_t gr_cnn_num_params(gr_cnn *cnn);
+int gr_cnn_get_params(gr_cnn *cnn, float *h_out);
+int gr_cnn_set_params(gr_cnn *cnn, const float *h_in);
+int gr_cnn_forward(gr_cnn *cnn, const float *d_in, float *d_out);
+/* loss and gradients (host, parameter layout) without an update */
+int gr_cnn_grads(gr_cnn *cnn, const float *d_in, const float *d_target, float *h_grads, float *h_loss);
+int gr_cnn_train_step(gr_cnn *cnn, const float *d_in, const float *d_target, float lr, float *h_loss);
+/* C = A * B (row-major bf16 A: M x K, B: K x N; f32 C), k range split over `splits` blocks */
+int gr_cnn_gemm_test(int M, int N, int K, const void *d_a, const void *d_b, float *d_c, int splits);
+
 #ifdef __cplusplus
 }
 #endif
