@@ -56,6 +56,8 @@ SIGNATURES = {
     "gr_get_fenwick": (_I, [_P, _P]),
     "gr_stream": (_P, [_P]),
     "gr_launch_count": (_I64, [_P]),
+    "gr_features": (_I, [_P, _P, C.c_float, _P]),
+    "gr_set_lookahead": (_I, [_P, _P, C.c_float, _P]),
     "gr_tune_set": (_I, [_P, _I, _I]),
     "gr_tune_get": (_I, [_P, _I, _P]),
     "gr_profile_enable": (_I, [_P, _I]),

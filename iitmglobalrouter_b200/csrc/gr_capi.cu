@@ -82,6 +82,10 @@ struct gr_ctx {
     cudaStream_t side[3] = {};       // concurrent Boruvka size classes (graph branches when captured)
     cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
     float *d_dlut = nullptr;  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
+    // lookahead cost mode: predicted further demand per cell and its weight
+    float *d_pred = nullptr;
+    float la_beta = 0.0f;
+    bool la_on = false;
     // tracks that gained marked cells in a batch: bitmap, list of first cells
     uint32_t *d_tbits = nullptr;
     int32_t *d_tlist = nullptr;
@@ -433,7 +437,7 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     if (blocks > (int64_t)c->sm_count * 8) blocks = (int64_t)c->sm_count * 8;
     k_track_commit<<<(int)blocks, kTrackWarps * 32, track_smem(c->track_cap), s>>>(
         c->g, c->d_tlist, c->d_list_count, c->d_mark, c->d_tbits, c->d_capr, c->d_dlut, c->d_fen, c->d_gpos,
-        c->d_gdel, c->track_cap);
+        c->d_gdel, c->track_cap, c->la_on ? c->d_pred : nullptr, c->la_beta);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -509,6 +513,19 @@ void free_buf(DevBuf &b) {
 void drop_graph(gr_ctx *c) {
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph = GraphCache{};
+}
+
+// Fenwick trees from the current capacities, with the plain or the lookahead cost
+int rebuild_fenwick(gr_ctx *c, cudaStream_t s) {
+    int pi = prof_begin(c, s);
+    if (c->la_on)
+        k_fen_init_la<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_pred,
+                                                                     c->la_beta, c->d_fen);
+    else
+        k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
+    prof_end(c, s, pi, GR_K_FEN_INIT);
+    GR_CK(cudaGetLastError());
+    return GR_OK;
 }
 
 }  // namespace
@@ -634,6 +651,7 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_fen);
     cudaFree(c->d_lut);
     cudaFree(c->d_dlut);
+    cudaFree(c->d_pred);
     cudaFree(c->d_tbits);
     cudaFree(c->d_tlist);
     cudaFree(c->d_gpos);
@@ -678,11 +696,7 @@ int gr_reset(gr_ctx *c, void *stream) {
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
     GR_CK(cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s));
-    int pi = prof_begin(c, s);
-    k_fen_init<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_lut, c->d_fen);
-    prof_end(c, s, pi, GR_K_FEN_INIT);
-    GR_CK(cudaGetLastError());
-    return GR_OK;
+    return rebuild_fenwick(c, s);
 }
 
 int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins) {
@@ -1021,6 +1035,35 @@ int gr_get_fenwick(gr_ctx *c, float *h_out) {
 }
 
 void *gr_stream(gr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int gr_features(gr_ctx *c, float *d_feat, float scale, void *stream) {
+    if (!c || !d_feat) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    k_features<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_cap0, c->d_capr, scale,
+                                                               d_feat);
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+int gr_set_lookahead(gr_ctx *c, const float *d_pred, float beta, void *stream) {
+    if (!c || !(beta >= 0.0f)) return GR_ERR_ARG;
+    cudaStream_t s = pick(c, stream);
+    drop_graph(c);  // a captured plan holds the cost mode it was captured with
+    if (!d_pred || beta == 0.0f) {
+        c->la_on = false;
+        c->la_beta = 0.0f;
+    } else {
+        if (!c->d_pred && cudaMalloc(&c->d_pred, sizeof(float) * (size_t)c->csize) != cudaSuccess) {
+            cudaGetLastError();
+            return GR_ERR_NOMEM;
+        }
+        k_pred_to_cells<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, d_pred, c->d_pred);
+        GR_CK(cudaGetLastError());
+        c->la_on = true;
+        c->la_beta = beta;
+    }
+    return rebuild_fenwick(c, s);
+}
 
 int gr_tune_set(gr_ctx *c, int param, int value) {
     if (!c || param < 0 || param >= GR_TUNE_PARAMS) return GR_ERR_ARG;

@@ -153,10 +153,53 @@ __global__ void k_dlut(const float *__restrict__ lut, float *__restrict__ dlut) 
         dlut[c] = lut_inc(lut, c + kLutMin);
 }
 
+// Lookahead cost of a GCELL with remaining capacity c and predicted
+// further demand p: exp(-0.5 (c - beta p)), the reference's cost with the
+// capacity the remaining batches are expected to leave (no counterpart in
+// the reference; the plain cost keeps using the exact table)
+__device__ __forceinline__ float la_cost(int c, float p, float beta) { return expf(-0.5f * ((float)c - beta * p)); }
+
 // ---------------------------------------------------------------- Fenwick build
 // bit_util.hpp:56-74 builds each node by atomically adding every cell's cost
 // along its update path. Here each node is owned by one thread that adds the
 // costs of its range (i - lowbit(i), i] in ascending order from 0.
+// the same with the lookahead cost (pred in cell order)
+__global__ void k_fen_init_la(GridC g, int csize, const int32_t *__restrict__ capr, const float *__restrict__ pred,
+                              float beta, float *__restrict__ fen) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < csize; e += gridDim.x * blockDim.x) {
+        int z, x, y;
+        dec(g, e, z, x, y);
+        const int p = (z & 1) ? y : x;
+        const int32_t base = e - p;
+        const int i = p + 1;
+        float res = 0.0f;
+        for (int q = i - (i & -i) + 1; q <= i; q++)
+            res += la_cost(__ldg(capr + base + q - 1), __ldg(pred + base + q - 1), beta);
+        fen[e] = res;
+    }
+}
+
+// pred[enc(z, x, y)] = src[z][y][x] (the network's grid layout), clamped at 0
+__global__ void k_pred_to_cells(GridC g, int csize, const float *__restrict__ src, float *__restrict__ pred) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < csize; e += gridDim.x * blockDim.x) {
+        int z, x, y;
+        dec(g, e, z, x, y);
+        pred[e] = fmaxf(src[((int64_t)z * g.Y + y) * g.X + x], 0.0f);
+    }
+}
+
+// network input: feat[z][y][x] = demand * scale, feat[Z + z][y][x] = capacity * scale
+__global__ void k_features(GridC g, int csize, const int32_t *__restrict__ cap0, const int32_t *__restrict__ capr,
+                           float scale, float *__restrict__ feat) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < csize; e += gridDim.x * blockDim.x) {
+        int z, x, y;
+        dec(g, e, z, x, y);
+        const int64_t o = ((int64_t)z * g.Y + y) * g.X + x;
+        feat[o] = (float)(cap0[e] - capr[e]) * scale;
+        feat[(int64_t)csize + o] = (float)cap0[e] * scale;
+    }
+}
+
 __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr, const float *__restrict__ lut,
                            float *__restrict__ fen) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < csize; e += gridDim.x * blockDim.x) {
@@ -1027,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
                                                       uint32_t *tbits, int32_t *__restrict__ capr,
                                                       const float *__restrict__ dlut, float *__restrict__ fen,
                                                       int32_t *__restrict__ gpos, float *__restrict__ gdel,
-                                                      int cap) {
+                                                      int cap, const float *__restrict__ pred, float beta) {
     extern __shared__ int32_t tsm[];  // per warp: cap positions, then cap increments
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
@@ -1076,7 +1119,12 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
                     b &= b - 1;
                     const int cv = capr[e];
                     P[k] = e - base;
-                    D[k] = __ldg(dlut + (cv < kLutMin ? 0 : (cv > kLutMax + 1 ? kLutMax + 1 - kLutMin : cv - kLutMin)));
+                    if (pred) {
+                        const float pe = __ldg(pred + e);
+                        D[k] = la_cost(cv - 1, pe, beta) - la_cost(cv, pe, beta);
+                    } else {
+                        D[k] = __ldg(dlut + (cv < kLutMin ? 0 : (cv > kLutMax + 1 ? kLutMax + 1 - kLutMin : cv - kLutMin)));
+                    }
                     capr[e] = cv - 1;
                     k++;
                 }

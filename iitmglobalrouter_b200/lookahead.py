@@ -89,3 +89,162 @@ class LookaheadNet:
         check(self._lib.gr_cnn_train_step(self._h, x.data_ptr(), target.data_ptr(), C.c_float(lr), ptr(loss)),
               "gr_cnn_train_step")
         return float(loss[0])
+
+
+# ---------------------------------------------------------------- data, training, routing
+
+SCALE = 1.0 / 16  # demand and capacity units fed to the network
+
+
+def _router_for(design, device=0):
+    from .router import Router
+
+    dims = design.dims
+    R = Router(dims["X"], dims["Y"], dims["Z"], design.caps(), device=device)
+    ofs, pins = design.nets()
+    R.set_nets(ofs, pins)
+    return R
+
+
+def snapshot_samples(design, fracs=(0.10, 0.25, 0.50, 0.75), num_xdim_parts=4, device=0):
+    """Training pairs from one plain route of the design: for each fraction f,
+    the network input after round(f * batches) batches and the demand the
+    remaining batches add (both scaled by SCALE). CUDA tensors."""
+    import torch
+
+    bofs, ids = design.batch(num_xdim_parts)
+    R = _router_for(design, device)
+    R.plan_set(bofs, ids)
+    nb = len(bofs) - 1
+    mst = torch.empty(R.plan_slots, dtype=torch.int64, device=f"cuda:{device}")
+    pat = torch.empty(R.plan_slots, dtype=torch.int32, device=f"cuda:{device}")
+    R.set_lookahead(None)
+    R.reset()
+    feats, prev = [], 0
+    for f in fracs:
+        b = min(nb, max(prev, int(round(f * nb))))
+        R.route_plan(mst, pat, b0=prev, b1=b)
+        feats.append(R.features(SCALE))
+        prev = b
+    R.route_plan(mst, pat, b0=prev, b1=nb)
+    final = R.features(SCALE)
+    R.sync()
+    Z = R.Z
+    out = [(x, (final[:Z] - x[:Z]).contiguous()) for x in feats]
+    R.close()
+    return out
+
+
+def train(net, samples, epochs=20, lr=1e-3, seed=0, log=None):
+    """Adam on the samples, one sample per step, shuffled every epoch; returns the mean loss per epoch."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    for ep in range(epochs):
+        order = rng.permutation(len(samples))
+        tot = 0.0
+        for i in order:
+            x, t = samples[i]
+            tot += net.train_step(x, t, lr)
+        hist.append(tot / len(samples))
+        if log:
+            log(f"epoch {ep}: loss {hist[-1]:.5f}")
+    return hist
+
+
+def route_lookahead(R, net, mst, pat, n_batches, every=64, beta=1.0):
+    """Route the plan from reset with the lookahead cost: before every block
+    of `every` batches the network predicts, from the current demand and
+    capacity, the demand still to come, and the cost becomes
+    exp(-0.5 (cap_remaining - beta * prediction)). beta = 0 routes plainly."""
+    R.set_lookahead(None)
+    R.reset()
+    for b0 in range(0, n_batches, every):
+        b1 = min(n_batches, b0 + every)
+        if beta > 0:
+            pred = (net.forward(R.features(SCALE)) * (1.0 / SCALE)).contiguous()
+            R.set_lookahead(pred, beta)
+        R.route_plan(mst, pat, b0=b0, b1=b1)
+    R.sync()
+    R.set_lookahead(None)
+
+
+def quality(design, R, mst, pat):
+    """Total overflow, overflowed GCELLs, demand, wirelength and vias of a routed plan."""
+    q = design.evaluate(R.demand())
+    import os
+
+    wl, vias = design.write_routes(os.devnull, mst.cpu().numpy(), pat.cpu().numpy(), merge=True, rseg=True,
+                                   ppatch=True, threads=8)
+    return dict(q, wirelength=wl, vias=vias)
+
+
+def evaluate(design, net, betas=(0.0, 0.5, 1.0, 2.0), every=64, num_xdim_parts=4, device=0):
+    """{beta: quality} of the design routed with each lookahead weight (0 = plain)."""
+    import torch
+
+    bofs, ids = design.batch(num_xdim_parts)
+    R = _router_for(design, device)
+    R.plan_set(bofs, ids)
+    mst = torch.empty(R.plan_slots, dtype=torch.int64, device=f"cuda:{device}")
+    pat = torch.empty(R.plan_slots, dtype=torch.int32, device=f"cuda:{device}")
+    out = {}
+    for beta in betas:
+        route_lookahead(R, net, mst, pat, len(bofs) - 1, every=every, beta=beta)
+        out[beta] = quality(design, R, mst, pat)
+    R.close()
+    return out
+
+
+def main(argv=None):
+    """Train the lookahead network on router snapshots of seeded 400x400x9
+    designs and compare plain and lookahead routing on held-out seeds.
+
+        python -m iitmglobalrouter_b200.lookahead --designs 50 --epochs 20 --out weights.npy --report report.json
+    """
+    import argparse
+    import json
+    import time
+
+    from .router import Design
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--designs", type=int, default=50)
+    ap.add_argument("--nets", type=int, default=0, help="nets per design (0: the configuration's)")
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--hidden", type=int, default=32)
+    ap.add_argument("--layers", type=int, default=4)
+    ap.add_argument("--every", type=int, default=64)
+    ap.add_argument("--betas", default="0,0.25,0.5,1,2")
+    ap.add_argument("--test-seeds", default="1001,1002,1003")
+    ap.add_argument("--out", default="")
+    ap.add_argument("--report", default="")
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    samples = []
+    for s in range(1, a.designs + 1):
+        samples += snapshot_samples(Design.generate(a.config, seed=s, n_nets=a.nets))
+    d0 = Design.generate(a.config, seed=1, n_nets=a.nets).dims
+    t1 = time.time()
+    net = LookaheadNet(2 * d0["Z"], d0["Z"], d0["Y"], d0["X"], hidden=a.hidden, n_layers=a.layers, seed=7)
+    hist = train(net, samples, epochs=a.epochs, lr=a.lr, log=print)
+    t2 = time.time()
+    if a.out:
+        np.save(a.out, net.get_params())
+    betas = [float(b) for b in a.betas.split(",")]
+    results = {}
+    for s in [int(x) for x in a.test_seeds.split(",")]:
+        results[s] = evaluate(Design.generate(a.config, seed=s, n_nets=a.nets), net, betas=betas, every=a.every)
+        print(s, json.dumps(results[s]))
+    rep = {"config": a.config, "designs": a.designs, "samples": len(samples), "epochs": a.epochs, "lr": a.lr,
+           "hidden": a.hidden, "layers": a.layers, "every": a.every, "loss": hist, "data_s": t1 - t0,
+           "train_s": t2 - t1, "results": {str(k): {str(b): v for b, v in r.items()} for k, r in results.items()}}
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump(rep, f, indent=1)
+    return rep
+
+
+if __name__ == "__main__":
+    main()

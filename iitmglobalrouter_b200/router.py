@@ -207,6 +207,28 @@ class Router:
                                              len(batch_ofs) - 1, ptr(batch_ofs), ptr(net_ids), ptr(mst_out),
                                              ptr(pat_out), 0), "gr_route_design_host")
 
+    # ---------------------------------------------------------- lookahead
+    def features(self, scale: float = 1.0 / 16):
+        """Network input from the current state: (2Z, Y, X) CUDA float32."""
+        import torch
+
+        out = torch.empty((2 * self.Z, self.Y, self.X), dtype=torch.float32, device=f"cuda:{self.device}")
+        torch.cuda.current_stream(self.device).synchronize()  # out allocated and free to write
+        check(self._lib.gr_features(self._h, out.data_ptr(), C.c_float(scale), None), "gr_features")
+        check(self._lib.gr_sync(self._h), "gr_sync")  # written before other streams read it
+        return out
+
+    def set_lookahead(self, pred=None, beta: float = 0.0):
+        """pred: (Z, Y, X) CUDA float32 predicted further demand, or None for the plain cost."""
+        if pred is not None:
+            import torch
+
+            assert pred.is_cuda and pred.dtype == torch.float32 and pred.is_contiguous()
+            assert tuple(pred.shape) == (self.Z, self.Y, self.X)
+            torch.cuda.current_stream(self.device).synchronize()  # pred complete before this stream reads it
+        check(self._lib.gr_set_lookahead(self._h, pred.data_ptr() if pred is not None else None, C.c_float(beta),
+                                         None), "gr_set_lookahead")
+
     # ---------------------------------------------------------- launch shapes
     def tune_set(self, param: int, value: int):
         check(self._lib.gr_tune_set(self._h, param, value), "gr_tune_set")

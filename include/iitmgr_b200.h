@@ -178,6 +178,17 @@ int64_t gr_launch_count(gr_ctx *ctx);
 #define GR_K_MST_WARP 8
 #define GR_K_MST_LARGE 9
 #define GR_PROF_KINDS 10
+/* Congestion lookahead (no counterpart in the reference). gr_features
+ * writes the network input from the current state: d_feat[z][y][x] =
+ * demand * scale, d_feat[Z + z][y][x] = capacity * scale (2Z x Y x X f32,
+ * device). gr_set_lookahead switches the GCELL cost to
+ * exp(-0.5 (cap_remaining - beta * pred)) with d_pred[z][y][x] the predicted
+ * further demand (Z x Y x X f32, device; negative values count as 0) and
+ * rebuilds the Fenwick trees from the current capacities; d_pred == NULL or
+ * beta == 0 returns to the exact table cost of the reference. */
+int gr_features(gr_ctx *ctx, float *d_feat, float scale, void *stream);
+int gr_set_lookahead(gr_ctx *ctx, const float *d_pred, float beta, void *stream);
+
 /* Launch shapes of the Boruvka size classes (results do not depend on them;
  * the autotuner in iitmglobalrouter_b200/tune.py picks them per GPU and Z). */
 #define GR_TUNE_MST_MID_THREADS 0      /* threads per CTA, nets of 33..128 pins  */
