@@ -106,3 +106,20 @@ def test_snapshot_train_and_route(cuda):
     R.route_plan(mst, pat)
     R.sync()
     assert plain == lookahead.quality(d, R, mst, pat)
+
+
+def test_trained_network_lowers_overflow(cuda):
+    """The shipped network (trained on snapshots of 50 seeded 400x400x9
+    designs) on a design it never saw: lower total overflow than the plain
+    cost at no more than 1 % more wirelength."""
+    from pathlib import Path
+
+    params = np.load(Path(lookahead.__file__).with_name("lookahead_c2.npy"))
+    d = gr.Design.generate(2, seed=1004)
+    dims = d.dims
+    net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=32, n_layers=4)
+    net.set_params(params)
+    res = lookahead.evaluate(d, net, betas=(0.0, 0.5), every=16)
+    plain, la = res[0.0], res[0.5]
+    assert la["overflow"] < plain["overflow"]
+    assert la["wirelength"] <= 1.01 * plain["wirelength"]
