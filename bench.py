@@ -77,6 +77,53 @@ def kernel_units(ofs, ids, committed):
     }
 
 
+def learned_quality(d, R, mst, pat, n_batches, dims):
+    """Quality of the design routed with the lookahead cost, when the package
+    ships a network for this layer count (lookahead_z<Z>.npy with its
+    lookahead_z<Z>.json report naming beta and the prediction interval);
+    the route's own time is reported beside it (not part of `value`)."""
+    import torch
+
+    from iitmglobalrouter_b200 import lookahead
+
+    base = ROOT / "iitmglobalrouter_b200" / f"lookahead_z{dims['Z']}"
+    if not base.with_suffix(".npy").exists():
+        return None
+    rep = json.loads(base.with_suffix(".json").read_text())
+    beta, every = float(rep["beta"]), int(rep["every"])
+    net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
+                                 n_layers=rep["layers"])
+    net.set_params(np.load(base.with_suffix(".npy")))
+    t0 = time.perf_counter()
+    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    out = lookahead.quality(d, R, mst, pat)
+    out.update(beta=beta, every=every, route_ms=dt * 1e3, weights=base.with_suffix(".npy").name)
+    R.reset()
+    return out
+
+
+def learned_quality_small():
+    """Plain against lookahead routing of a held-out 400x400x9 design (150 K
+    nets, seed 1001) with the package's network for 9 layers."""
+    from iitmglobalrouter_b200 import Design, lookahead
+
+    base = ROOT / "iitmglobalrouter_b200" / "lookahead_z9"
+    if not base.with_suffix(".npy").exists():
+        return None
+    rep = json.loads(base.with_suffix(".json").read_text())
+    d = Design.generate(2, seed=1001)
+    dims = d.dims
+    net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
+                                 n_layers=rep["layers"])
+    net.set_params(np.load(base.with_suffix(".npy")))
+    res = lookahead.evaluate(d, net, betas=(0.0, float(rep["beta"])), every=int(rep["every"]))
+    net.close()
+    return {"plain": res[0.0], "learned": res[float(rep["beta"])], "beta": float(rep["beta"]),
+            "every": int(rep["every"]), "seed": 1001}
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -284,6 +331,8 @@ def main():
     if not replicas.replicas_agree(replicas.digest(mst_h, pat_h, demand), dist, dev):
         raise SystemExit("replicas routed the design differently")
     wl, vias = d.write_routes(os.devnull, mst_h, pat_h, merge=True, rseg=True, ppatch=True, threads=8)
+    learned = learned_quality(d, R, mst, pat, len(bofs) - 1, dims)
+    learned_c2 = learned_quality_small()
 
     # per-kernel breakdown: one profiled step (events around each launch)
     R.reset()
@@ -367,8 +416,10 @@ def main():
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
         "gpu_launches": int(launches),
         "clocks": clocks,
-        "quality": {"overflow": q["overflow"], "overflow_cells": q["overflow_cells"], "demand": q["demand"],
-                    "wirelength": wl, "vias": vias},
+        "quality": {"plain": {"overflow": q["overflow"], "overflow_cells": q["overflow_cells"], "demand": q["demand"],
+                              "wirelength": wl, "vias": vias},
+                    "learned": learned,
+                    "400x400x9": learned_c2},
     }
     print(json.dumps(out), flush=True)
 

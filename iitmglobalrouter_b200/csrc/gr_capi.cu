@@ -615,8 +615,11 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         cudaMemset(c->d_list_count, 0, 16) ||
         cudaMemset(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)))
         return fail(GR_ERR_CUDA);
+    // A function attribute holds for the whole process, not this context:
+    // set it to the most any context launches with, so that a context for a
+    // smaller grid created later cannot lower it under a larger one's needs.
     if (cudaFuncSetAttribute(k_track_commit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)track_smem(c->track_cap)) != cudaSuccess)
+                             (int)track_smem(kTrackCapMax)) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     k_dlut<<<(kLutMax - kLutMin + 2 + 255) / 256, 256, 0, c->stream>>>(c->d_lut, c->d_dlut);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);

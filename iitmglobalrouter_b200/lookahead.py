@@ -220,15 +220,20 @@ def main(argv=None):
     ap.add_argument("--test-seeds", default="1001,1002,1003")
     ap.add_argument("--out", default="")
     ap.add_argument("--report", default="")
+    ap.add_argument("--weights", default="", help="evaluate these parameters instead of training")
     a = ap.parse_args(argv)
     t0 = time.time()
-    samples = []
-    for s in range(1, a.designs + 1):
-        samples += snapshot_samples(Design.generate(a.config, seed=s, n_nets=a.nets))
     d0 = Design.generate(a.config, seed=1, n_nets=a.nets).dims
-    t1 = time.time()
     net = LookaheadNet(2 * d0["Z"], d0["Z"], d0["Y"], d0["X"], hidden=a.hidden, n_layers=a.layers, seed=7)
-    hist = train(net, samples, epochs=a.epochs, lr=a.lr, log=print)
+    samples, hist = [], []
+    if a.weights:
+        net.set_params(np.load(a.weights))
+    else:
+        for s in range(1, a.designs + 1):
+            samples += snapshot_samples(Design.generate(a.config, seed=s, n_nets=a.nets))
+    t1 = time.time()
+    if not a.weights:
+        hist = train(net, samples, epochs=a.epochs, lr=a.lr, log=print)
     t2 = time.time()
     if a.out:
         np.save(a.out, net.get_params())

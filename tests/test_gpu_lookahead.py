@@ -114,7 +114,7 @@ def test_trained_network_lowers_overflow(cuda):
     cost at no more than 1 % more wirelength."""
     from pathlib import Path
 
-    params = np.load(Path(lookahead.__file__).with_name("lookahead_c2.npy"))
+    params = np.load(Path(lookahead.__file__).with_name("lookahead_z9.npy"))
     d = gr.Design.generate(2, seed=1004)
     dims = d.dims
     net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=32, n_layers=4)

@@ -335,3 +335,19 @@ def test_route_design_host_end_to_end(cuda):
     R.route_design_host(ofs, pins, bofs, ids, mst, mp)
     assert np.array_equal(mst, mst_c) and np.array_equal(mp, mp_c)
     assert np.array_equal(R.demand(), g.demand())
+
+
+def test_contexts_of_different_sizes_coexist(cuda):
+    """A context for a small grid created after one for a larger grid leaves
+    the larger one routable (kernel attributes are process-wide)."""
+    d = gr.Design.generate_custom(300, 300, 3, 2, 6, 400, seed=1)
+    X, Y, Z, cap, ofs, pins = design_arrays(d)
+    bofs, ids = d.batch(4)
+    big = gr.Router(X, Y, Z, cap)
+    big.set_nets(ofs, pins)
+    a, _ = route_all_gpu(big, ofs, bofs, ids, "plan")
+    small = gr.Router(16, 16, 3, np.ones(16 * 16 * 3, np.int32))
+    big.reset()
+    b, _ = route_all_gpu(big, ofs, bofs, ids, "plan")
+    assert big.status() == 0 and np.array_equal(a, b)
+    small.close()
