@@ -586,8 +586,12 @@ void make_batches(const Design &d, int K, Plan &plan) {
     plan.net_ids.clear();
     plan.net_ids.reserve(N);
     int rem = N;
-    BoxIndex idx;
-    idx.init(d.X, d.Y);
+    // one intersection index per bucket: the buckets' greedy passes are
+    // independent and run in parallel (as the reference's OpenMP loop over
+    // buckets does); their picks are joined in bucket order
+    std::vector<BoxIndex> idxs(K + 1);
+    for (auto &ix : idxs) ix.init(d.X, d.Y);
+    std::vector<std::vector<int>> picked(K + 1);
     struct RM {
         int key;
         int id;
@@ -629,28 +633,31 @@ void make_batches(const Design &d, int K, Plan &plan) {
             }
         // per bucket: sort by half perimeter, greedy non-overlap (:214-234)
         batch.clear();
-        struct RH {
-            int key;
-            int id;
-        };
-        std::vector<RH> rh;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nparts)
         for (int p = 0; p < nparts; p++) {
-            rh.resize(pick[p].size());
+            struct RH {
+                int key;
+                int id;
+            };
+            std::vector<RH> rh(pick[p].size());
             for (size_t i = 0; i < pick[p].size(); i++) {
                 const Box &b = bx[pick[p][i]];
                 rh[i] = {(b.maxx - b.minx + 1) + (b.maxy - b.miny + 1), pick[p][i]};
             }
             std::sort(rh.begin(), rh.end(), [](const RH &a, const RH &b) { return a.key < b.key; });
+            BoxIndex &idx = idxs[p];
             idx.reset();
+            picked[p].clear();
             for (const RH &h : rh) {
                 const Box &b = bx[h.id];
                 if (!idx.hits(b)) {
                     idx.insert(b);
-                    batch.push_back(h.id);
-                    vis[h.id] = 1;
+                    picked[p].push_back(h.id);
+                    vis[h.id] = 1;  // each net lies in one bucket: no two threads write one entry
                 }
             }
         }
+        for (int p = 0; p < nparts; p++) batch.insert(batch.end(), picked[p].begin(), picked[p].end());
         // compaction of the remaining ids (net_part.hpp:326-337)
         int id = 0, fid = 0;
         while (id < rem) {
