@@ -90,16 +90,16 @@ def learned_quality(d, R, mst, pat, n_batches, dims):
     if not base.with_suffix(".npy").exists():
         return None
     rep = json.loads(base.with_suffix(".json").read_text())
-    beta, every = float(rep["beta"]), int(rep["every"])
+    beta, every, mode = float(rep["beta"]), int(rep["every"]), rep.get("mode", "demand")
     net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
                                  n_layers=rep["layers"])
     net.set_params(np.load(base.with_suffix(".npy")))
     t0 = time.perf_counter()
-    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta)
+    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta, mode=mode)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     out = lookahead.quality(d, R, mst, pat)
-    out.update(beta=beta, every=every, route_ms=dt * 1e3, weights=base.with_suffix(".npy").name)
+    out.update(beta=beta, every=every, mode=mode, route_ms=dt * 1e3, weights=base.with_suffix(".npy").name)
     R.reset()
     return out
 
@@ -118,7 +118,8 @@ def learned_quality_small():
     net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
                                  n_layers=rep["layers"])
     net.set_params(np.load(base.with_suffix(".npy")))
-    res = lookahead.evaluate(d, net, betas=(0.0, float(rep["beta"])), every=int(rep["every"]))
+    res = lookahead.evaluate(d, net, betas=(0.0, float(rep["beta"])), every=int(rep["every"]),
+                             mode=rep.get("mode", "demand"))
     net.close()
     return {"plain": res[0.0], "learned": res[float(rep["beta"])], "beta": float(rep["beta"]),
             "every": int(rep["every"]), "seed": 1001}

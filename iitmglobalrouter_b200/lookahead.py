@@ -151,18 +151,26 @@ def train(net, samples, epochs=20, lr=1e-3, seed=0, log=None):
     return hist
 
 
-def route_lookahead(R, net, mst, pat, n_batches, every=64, beta=1.0):
+def route_lookahead(R, net, mst, pat, n_batches, every=64, beta=1.0, mode="demand"):
     """Route the plan from reset with the lookahead cost: before every block
     of `every` batches the network predicts, from the current demand and
     capacity, the demand still to come, and the cost becomes
-    exp(-0.5 (cap_remaining - beta * prediction)). beta = 0 routes plainly."""
+    exp(-0.5 (cap_remaining - beta * p)) with p the prediction (mode
+    "demand") or only its part beyond the capacity then remaining (mode
+    "excess": cells expected to overflow). beta = 0 routes plainly."""
+    import torch
+
     R.set_lookahead(None)
     R.reset()
+    Z = R.Z
     for b0 in range(0, n_batches, every):
         b1 = min(n_batches, b0 + every)
         if beta > 0:
-            pred = (net.forward(R.features(SCALE)) * (1.0 / SCALE)).contiguous()
-            R.set_lookahead(pred, beta)
+            f = R.features(SCALE)
+            pred = net.forward(f) * (1.0 / SCALE)
+            if mode == "excess":
+                pred = torch.relu(pred - (f[Z:] - f[:Z]) * (1.0 / SCALE))
+            R.set_lookahead(pred.contiguous(), beta)
         R.route_plan(mst, pat, b0=b0, b1=b1)
     R.sync()
     R.set_lookahead(None)
@@ -178,7 +186,7 @@ def quality(design, R, mst, pat):
     return dict(q, wirelength=wl, vias=vias)
 
 
-def evaluate(design, net, betas=(0.0, 0.5, 1.0, 2.0), every=64, num_xdim_parts=4, device=0):
+def evaluate(design, net, betas=(0.0, 0.5, 1.0, 2.0), every=64, num_xdim_parts=4, device=0, mode="demand"):
     """{beta: quality} of the design routed with each lookahead weight (0 = plain)."""
     import torch
 
@@ -189,7 +197,7 @@ def evaluate(design, net, betas=(0.0, 0.5, 1.0, 2.0), every=64, num_xdim_parts=4
     pat = torch.empty(R.plan_slots, dtype=torch.int32, device=f"cuda:{device}")
     out = {}
     for beta in betas:
-        route_lookahead(R, net, mst, pat, len(bofs) - 1, every=every, beta=beta)
+        route_lookahead(R, net, mst, pat, len(bofs) - 1, every=every, beta=beta, mode=mode)
         out[beta] = quality(design, R, mst, pat)
     R.close()
     return out
@@ -221,6 +229,7 @@ def main(argv=None):
     ap.add_argument("--out", default="")
     ap.add_argument("--report", default="")
     ap.add_argument("--weights", default="", help="evaluate these parameters instead of training")
+    ap.add_argument("--mode", default="demand", choices=["demand", "excess"])
     a = ap.parse_args(argv)
     t0 = time.time()
     d0 = Design.generate(a.config, seed=1, n_nets=a.nets).dims
@@ -240,9 +249,10 @@ def main(argv=None):
     betas = [float(b) for b in a.betas.split(",")]
     results = {}
     for s in [int(x) for x in a.test_seeds.split(",")]:
-        results[s] = evaluate(Design.generate(a.config, seed=s, n_nets=a.nets), net, betas=betas, every=a.every)
+        results[s] = evaluate(Design.generate(a.config, seed=s, n_nets=a.nets), net, betas=betas, every=a.every,
+                              mode=a.mode)
         print(s, json.dumps(results[s]))
-    rep = {"config": a.config, "designs": a.designs, "samples": len(samples), "epochs": a.epochs, "lr": a.lr,
+    rep = {"config": a.config, "mode": a.mode, "designs": a.designs, "samples": len(samples), "epochs": a.epochs, "lr": a.lr,
            "hidden": a.hidden, "layers": a.layers, "every": a.every, "loss": hist, "data_s": t1 - t0,
            "train_s": t2 - t1, "results": {str(k): {str(b): v for b, v in r.items()} for k, r in results.items()}}
     if a.report:
