@@ -101,7 +101,7 @@ struct gr_ctx {
     GraphCache graph;
     int64_t launches = 0;
     int mst_smem_max = 0;
-    int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129};  // GR_TUNE_* values (best measured on B200, Z = 10)
+    int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
     int levels = 0;  // nodes on the longest Fenwick update path: 1 + floor(log2(max(X, Y)))
     // optional per-kernel timing (CUDA events around every launch)
     bool profiling = false;
@@ -317,10 +317,27 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
     if (v.n_pairs > 0) {
         int pi = prof_begin(c, s);
         const int grid = grid_for(c, v.n_pairs, 16);
-#define GR_LPAT_Z(ZV)                                                                                 \
-    case ZV:                                                                                          \
-        k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat, mst, \
-                                               dist);                                                   \
+        // warps per group of 32 pairs: 4 when one thread per pair would fill
+        // fewer than half of the SMs (measured: -3 us per batch there, slower
+        // as soon as the batch fills the GPU)
+        int split = c->tune[GR_TUNE_LPAT_SPLIT];
+        if (split == 0) {
+            const int64_t blocks1 = (v.n_pairs + kThreads - 1) / kThreads;
+            split = 2 * blocks1 < c->sm_count ? 4 : 1;
+        }
+        const int64_t gs = (v.n_pairs + kThreads / split - 1) / (kThreads / split);
+        const int grid_s = (int)(gs < 16LL * c->sm_count ? gs : 16LL * c->sm_count);
+#define GR_LPAT_Z(ZV)                                                                                     \
+    case ZV:                                                                                              \
+        if (split == 4)                                                                                   \
+            k_lpat_zs<ZV, 4><<<grid_s, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, \
+                                                         ppat, mst, dist);                                \
+        else if (split == 2)                                                                              \
+            k_lpat_zs<ZV, 2><<<grid_s, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, \
+                                                         ppat, mst, dist);                                \
+        else                                                                                              \
+            k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat, \
+                                                   mst, dist);                                            \
         break;
         switch (c->g.Z) {
             GR_LPAT_Z(3) GR_LPAT_Z(4) GR_LPAT_Z(5) GR_LPAT_Z(6) GR_LPAT_Z(7) GR_LPAT_Z(8) GR_LPAT_Z(9)
@@ -1072,6 +1089,8 @@ int gr_tune_set(gr_ctx *c, int param, int value) {
     if (!c || param < 0 || param >= GR_TUNE_PARAMS) return GR_ERR_ARG;
     if (param == GR_TUNE_MST_CLUSTER_MIN_PINS) {
         if (value != 0 && (value <= kMstMidPins || value > GR_MAX_PINS)) return GR_ERR_ARG;
+    } else if (param == GR_TUNE_LPAT_SPLIT) {
+        if (value != 0 && value != 1 && value != 2 && value != 4) return GR_ERR_ARG;
     } else if (value < 64 || value > 1024 || value % 32) {
         return GR_ERR_ARG;
     }

@@ -642,9 +642,13 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
 // each the same single FP32 subtraction the reference's range query makes
 // (bit_util.hpp:36-38). With Z a compile-time constant the 6Z values stay
 // in registers and every pattern is summed in path order from them.
-template <int ZC>
-__device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
-                                          int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p) {
+// Patterns of the first-via layers via1 with (via1 - 1) % S == SUB (all of
+// them for S = 1): the lowest-cost valid pattern (best, bp; bp = -1 when no
+// valid pattern has a finite cost) and the lowest valid pattern id (first).
+template <int ZC, int S, int SUB>
+__device__ __forceinline__ void lpat_regs_part(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
+                                               int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p,
+                                               int &out_first) {
     constexpr int Z2 = (ZC + 1) / 2;
     float Pj[ZC], Pk[ZC], Pc1[ZC], Pc2[ZC], W1[ZC], W2[ZC];
     const int64_t nn = (int64_t)nx * ny;
@@ -673,6 +677,7 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, 
     int bp = -1, first = -1;
 #pragma unroll
     for (int via1 = 1; via1 < ZC; via1++) {
+        if ((via1 - 1) % S != SUB) continue;
         const bool even1 = (via1 & 1) == 0;
         float c0 = 0.0f;
 #pragma unroll
@@ -717,12 +722,22 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, 
             }
         }
     }
-    if (bp < 0) {
-        bp = first;
-        best = __int_as_float(0x7f800000);
-    }
     out_c = best;
     out_p = bp;
+    out_first = first;
+}
+
+// all patterns of the pair: the cheapest, ties to the lowest id; with no
+// finite-cost valid pattern, the lowest valid id at cost +inf
+template <int ZC>
+__device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
+                                          int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p) {
+    int first;
+    lpat_regs_part<ZC, 1, 0>(T, nx, ny, pj, pk, z1, z2, xj, yj, xk, yk, out_c, out_p, first);
+    if (out_p < 0) {
+        out_p = first;
+        out_c = __int_as_float(0x7f800000);
+    }
 }
 
 template <int ZC>
@@ -757,6 +772,90 @@ __global__ void __launch_bounds__(256, 2) k_lpat_z(GridC g, BatchView bv, const 
         cost[p] = c;
         pat[p] = (int16_t)cp;
         pin2_tree(bv, net, c, mst, dist);
+    }
+}
+
+// The same with S warps per group of 32 pairs (for batches too small to fill
+// the GPU one thread per pair): warp w evaluates the first-via layers of
+// subset w % S for pairs 32 (w / S) .. of the block's share, and the S
+// partial results are joined in shared memory -- the cheapest pattern over
+// all subsets, ties to the lowest id, else the lowest valid id at +inf.
+template <int ZC, int S, int SUB>
+__device__ __forceinline__ void lpat_sub(const float2 *T, int nx, int ny, int pj, int pk, int z1, int z2, int xj,
+                                         int yj, int xk, int yk, int sub, float &c, int &bp, int &first) {
+    if constexpr (SUB < S) {
+        if (sub == SUB) lpat_regs_part<ZC, S, SUB>(T, nx, ny, pj, pk, z1, z2, xj, yj, xk, yk, c, bp, first);
+        else lpat_sub<ZC, S, SUB + 1>(T, nx, ny, pj, pk, z1, z2, xj, yj, xk, yk, sub, c, bp, first);
+    }
+}
+
+template <int ZC, int S>
+__global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                                 Coords cd, const float *__restrict__ fen,
+                                                 const float2 *__restrict__ tab, float *__restrict__ cost,
+                                                 int16_t *__restrict__ pat, int64_t *__restrict__ mst,
+                                                 float *__restrict__ dist) {
+    static_assert(S == 2 || S == 4 || S == 8, "warps per pair group");
+    __shared__ float sc[8][32];
+    __shared__ int sp[8][32], sf[8][32];
+    const float inf = __int_as_float(0x7f800000);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, sub = w % S, pg = w / S;
+    constexpr int PPB = 32 * (8 / S);  // pairs per block and step
+    for (int64_t bb = (int64_t)blockIdx.x * PPB; bb < bv.n_pairs; bb += (int64_t)gridDim.x * PPB) {
+        const int64_t p0 = bb + (int64_t)pg * 32, p = p0 + lane;
+        float c = inf;
+        int bp = -1, first = -1;
+        int net = 0;
+        if (p0 < bv.n_pairs) {  // warp-uniform
+            net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
+                                  p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
+            if (p < bv.n_pairs) {
+                int j, k;
+                pair_decode(p - bv.pair_ofs[net], j, k);
+                const int32_t *np = pins + bv.pin_base[net];
+                int z1, x1, y1, z2, x2, y2;
+                dec(g, __ldg(np + j), z1, x1, y1);
+                dec(g, __ldg(np + k), z2, x2, y2);
+                const int nxy = bv.nxy[net];
+                if (nxy) {
+                    const int64_t pb = bv.pin_base[net];
+                    lpat_sub<ZC, S, 0>(tab + bv.tab_ofs[net], nxy >> 16, nxy & 0xffff, __ldg(cd.pxy + pb + j),
+                                       __ldg(cd.pxy + pb + k), z1, z2, x1, y1, x2, y2, sub, c, bp, first);
+                } else if (sub == 0) {
+                    DirectEv ev{fen, g, z1, x1, y1, z2, x2, y2, (x1 != x2 && y1 != y2)};
+                    int cp;
+                    lpat_argmin(ev, g, c, cp);
+                    first = cp;
+                    bp = c < inf ? cp : -1;
+                }
+            }
+        }
+        sc[w][lane] = c;
+        sp[w][lane] = bp;
+        sf[w][lane] = first;
+        __syncthreads();
+        if (sub == 0 && p < bv.n_pairs) {
+            float bc = inf;
+            int bbp = -1, bf = -1;
+#pragma unroll
+            for (int q = 0; q < S; q++) {
+                const float qc = sc[w + q][lane];
+                const int qp = sp[w + q][lane], qf = sf[w + q][lane];
+                if (qp >= 0 && (bbp < 0 || qc < bc || (qc == bc && qp < bbp))) {
+                    bc = qc;
+                    bbp = qp;
+                }
+                if (qf >= 0 && (bf < 0 || qf < bf)) bf = qf;
+            }
+            if (bbp < 0) {
+                bbp = bf;
+                bc = inf;
+            }
+            cost[p] = bc;
+            pat[p] = (int16_t)bbp;
+            pin2_tree(bv, net, bc, mst, dist);
+        }
+        __syncthreads();
     }
 }
 

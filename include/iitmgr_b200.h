@@ -196,8 +196,11 @@ int gr_set_lookahead(gr_ctx *ctx, const float *d_pred, float beta, void *stream)
 #define GR_TUNE_MST_CLUSTER_THREADS 2  /* threads per CTA of a cluster            */
 #define GR_TUNE_MST_CLUSTER_MIN_PINS 3 /* nets from this size use a cluster even
                                           when one CTA could hold them (0: never) */
-#define GR_TUNE_PARAMS 4
+#define GR_TUNE_LPAT_SPLIT 4           /* warps sharing a group of 32 pairs in the
+                                          L-pattern kernel: 1, 2, 4 (0: by batch size) */
+#define GR_TUNE_PARAMS 5
 int gr_tune_set(gr_ctx *ctx, int param, int value); /* threads: 64..1024, multiple of 32 */
+/* (results do not depend on any of them; the L-pattern split only on latency) */
 int gr_tune_get(gr_ctx *ctx, int param, int *value);
 
 int gr_profile_enable(gr_ctx *ctx, int on);

@@ -161,7 +161,7 @@ def test_brvsk_launch_shapes_do_not_change_results(cuda, tuning):
 
 def test_tune_rejects_bad_values(cuda):
     R = gr.Router(8, 8, 3, np.ones(192, np.int32))
-    for p, v in [(0, 48), (0, 2048), (1, 100), (3, 100), (3, 5000), (7, 512)]:
+    for p, v in [(0, 48), (0, 2048), (1, 100), (3, 100), (3, 5000), (4, 3), (4, 8), (7, 512)]:
         with pytest.raises(gr.GRError):
             R.tune_set(p, v)
 
@@ -351,3 +351,26 @@ def test_contexts_of_different_sizes_coexist(cuda):
     b, _ = route_all_gpu(big, ofs, bofs, ids, "plan")
     assert big.status() == 0 and np.array_equal(a, b)
     small.close()
+
+
+@pytest.mark.parametrize("split", [1, 2, 4])
+def test_lpattern_split_bitexact(cuda, split):
+    """The L-pattern kernel with the first-via layers of each pair shared by
+    1, 2 or 4 warps gives the oracle's routes (even and odd Z)."""
+    from iitmglobalrouter_b200._capi import GR_TUNE_LPAT_SPLIT
+
+    for config, n_nets, nb in ((1, 0, None), (2, 20000, 2)):
+        d = gr.Design.generate(config, seed=2, n_nets=n_nets)
+        X, Y, Z, cap, ofs, pins = design_arrays(d)
+        bofs, ids = d.batch(4)
+        if nb:
+            bofs, ids = bofs[: nb + 1], ids[: bofs[nb]]
+        g = oracle.Grid(X, Y, Z, cap)
+        rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=NT)
+        assert rc == 0
+        R = gr.Router(X, Y, Z, cap)
+        R.tune_set(GR_TUNE_LPAT_SPLIT, split)
+        R.set_nets(ofs, pins)
+        mst, mp = route_all_gpu(R, ofs, bofs, ids, "plan")
+        assert np.array_equal(mst, mst_c) and np.array_equal(mp, mp_c)
+        assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))

@@ -66,5 +66,7 @@ def test_candidates_are_valid_values(p):
     for v in tune.CANDIDATES[p]:
         if p == 3:
             assert v == 0 or 128 < v <= 4096
+        elif p == 4:
+            assert v in (0, 1, 2, 4)
         else:
             assert 64 <= v <= 1024 and v % 32 == 0
