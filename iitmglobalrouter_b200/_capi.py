@@ -28,6 +28,7 @@ GR_STATIC_MAX_NETS, GR_STATIC_MAX_PINS = 65536, 1024
 GR_PROF_KINDS = 10
 GR_TUNE_MST_MID_THREADS, GR_TUNE_MST_BIG_THREADS, GR_TUNE_MST_CLUSTER_THREADS, GR_TUNE_MST_CLUSTER_MIN_PINS = 0, 1, 2, 3
 GR_TUNE_LPAT_SPLIT = 4
+GR_LA_DEMAND, GR_LA_EXCESS = 0, 1
 GR_TUNE_PARAMS = 5
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
@@ -81,6 +82,8 @@ SIGNATURES = {
     "gr_cnn_create": (_I, [_PP, _I, _I, _I, _I, _I, _I, _I, _U64]),
     "gr_cnn_destroy": (_I, [_P]),
     "gr_cnn_num_params": (_I64, [_P]),
+    "gr_cnn_info": (_I, [_P, _P, _P, _P, _P, _P]),
+    "gr_route_design_lookahead_host": (_I, [_P, _P, C.c_int32, C.c_float, _I, _P, _P]),
     "gr_cnn_get_params": (_I, [_P, _P]),
     "gr_cnn_set_params": (_I, [_P, _P]),
     "gr_cnn_forward": (_I, [_P, _P, _P]),

@@ -74,6 +74,7 @@ struct gr_ctx {
     // per-call batch descriptor (device) + pinned staging
     DevBuf desc, pcost, ppat, tab, dist;
     DevBuf out_mst, out_pat;             // results of gr_route_design_host
+    DevBuf la_feat, la_out;              // network input and output of the lookahead route
     cudaStream_t copy_stream = nullptr;  // its result copies, overlapping the route
     cudaEvent_t ev_out = nullptr;
     void *h_stage = nullptr;
@@ -698,6 +699,8 @@ int gr_destroy(gr_ctx *c) {
     if (c->ev_out) cudaEventDestroy(c->ev_out);
     free_buf(c->out_mst);
     free_buf(c->out_pat);
+    free_buf(c->la_feat);
+    free_buf(c->la_out);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -1083,6 +1086,48 @@ int gr_set_lookahead(gr_ctx *c, const float *d_pred, float beta, void *stream) {
         c->la_beta = beta;
     }
     return rebuild_fenwick(c, s);
+}
+
+int gr_route_design_lookahead_host(gr_ctx *c, gr_cnn *cnn, int32_t every, float beta, int mode,
+                                   int64_t *h_mst_edges, int32_t *h_mst_pat) {
+    if (!c || !cnn || !h_mst_edges || every < 1 || !(beta >= 0.0f) || (mode != GR_LA_DEMAND && mode != GR_LA_EXCESS))
+        return GR_ERR_ARG;
+    if (c->plan.empty()) return GR_ERR_STATE;
+    int dev = -1, cin = 0, cout = 0, H = 0, W = 0;
+    int rc = gr_cnn_info(cnn, &dev, &cin, &cout, &H, &W);
+    if (rc) return rc;
+    if (dev != c->device || cin != 2 * c->g.Z || cout != c->g.Z || H != c->g.Y || W != c->g.X) return GR_ERR_ARG;
+    const int64_t slots = c->plan_slots, n = c->csize;
+    const int32_t nb = (int32_t)c->plan.size();
+    if ((rc = ensure(c->out_mst, sizeof(int64_t) * (slots + 1), c->stream)) ||
+        (rc = ensure(c->out_pat, sizeof(int32_t) * (slots + 1), c->stream)) ||
+        (rc = ensure(c->la_feat, sizeof(float) * 2 * n, c->stream)) ||
+        (rc = ensure(c->la_out, sizeof(float) * 2 * n, c->stream)))
+        return rc;
+    int64_t *mst = (int64_t *)c->out_mst.p;
+    int32_t *pat = (int32_t *)c->out_pat.p;
+    float *feat = (float *)c->la_feat.p, *out = (float *)c->la_out.p, *pred = out + n;
+    if ((rc = gr_set_lookahead(c, nullptr, 0.0f, nullptr)) || (rc = gr_reset(c, nullptr))) return rc;
+    for (int32_t b0 = 0; b0 < nb && !rc; b0 += every) {
+        const int32_t b1 = b0 + every < nb ? b0 + every : nb;
+        if (beta > 0.0f) {
+            if ((rc = gr_features(c, feat, 1.0f / 16.0f, nullptr))) break;
+            GR_CK(cudaStreamSynchronize(c->stream));  // the network reads on its own stream
+            if ((rc = gr_cnn_forward(cnn, feat, out))) break;
+            k_la_pred<<<grid_for(c, n, 16), kThreads, 0, c->stream>>>((int)n, out, feat, mode == GR_LA_EXCESS, pred);
+            GR_CK(cudaGetLastError());
+            if ((rc = gr_set_lookahead(c, pred, beta, nullptr))) break;
+        }
+        rc = gr_route_plan(c, b0, b1, mst, pat, 0, nullptr);
+    }
+    if (!rc) {
+        GR_CK(cudaMemcpyAsync(h_mst_edges, mst, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream));
+        if (h_mst_pat)
+            GR_CK(cudaMemcpyAsync(h_mst_pat, pat, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream));
+    }
+    const int sr = gr_sync(c);
+    const int lr = gr_set_lookahead(c, nullptr, 0.0f, nullptr);
+    return rc ? rc : (sr ? sr : lr);
 }
 
 int gr_tune_set(gr_ctx *c, int param, int value) {

@@ -425,6 +425,16 @@ int gr_cnn_destroy(gr_cnn *c) {
 
 int64_t gr_cnn_num_params(gr_cnn *c) { return c ? c->n_params : -1; }
 
+int gr_cnn_info(gr_cnn *c, int *device, int *in_channels, int *out_channels, int *H, int *W) {
+    if (!c) return GR_ERR_ARG;
+    if (device) *device = c->device;
+    if (in_channels) *in_channels = c->cin[0];
+    if (out_channels) *out_channels = c->cout[c->n_layers - 1];
+    if (H) *H = c->H;
+    if (W) *W = c->W;
+    return GR_OK;
+}
+
 int gr_cnn_get_params(gr_cnn *c, float *h_out) {
     if (!c || !h_out) return GR_ERR_ARG;
     CN_CK(cudaStreamSynchronize(c->stream));

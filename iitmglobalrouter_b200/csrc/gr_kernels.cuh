@@ -200,6 +200,17 @@ __global__ void k_features(GridC g, int csize, const int32_t *__restrict__ cap0,
     }
 }
 
+// the network's output (demand / 16) as predicted further demand: x 16, and
+// in excess mode only its part beyond the remaining capacity (from the
+// input features: demand / 16 then capacity / 16)
+__global__ void k_la_pred(int n, const float *__restrict__ out, const float *__restrict__ feat, int excess,
+                          float *__restrict__ pred) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float p = out[i] * 16.0f;
+        pred[i] = excess ? fmaxf(p - (feat[n + i] - feat[i]) * 16.0f, 0.0f) : p;
+    }
+}
+
 __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr, const float *__restrict__ lut,
                            float *__restrict__ fen) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < csize; e += gridDim.x * blockDim.x) {

@@ -12,6 +12,12 @@
 //   -device d                    CUDA device (default 0)
 //   -report F                    JSON report: timings, nets/s, overflow, WL, vias
 //   -graph                       route the plan as one captured CUDA graph
+//   -lookahead F.npy             route with the learned congestion lookahead:
+//                                network parameters (float32 .npy); its
+//                                settings come from F.json beside it when
+//                                present (keys mode, beta, every, hidden,
+//                                layers) and from these flags, which win:
+//   -la_mode demand|excess  -la_beta b  -la_every k  -la_hidden h  -la_layers l
 // Unknown flags are ignored (as the reference does). -rbt_part, -ord_part,
 // -upd_ispd24_net_file and running without -bit_pmodel select reference modes
 // this tool does not provide; it stops with a message.
@@ -19,6 +25,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -31,7 +39,70 @@ struct Args {
     bool new_fmt = false, bit_pmodel = false, batch_part = false, wrt_mrg = false, rseg = false, ppatch = false;
     bool graph = false, rbt = false, ord = false, upd24 = false;
     int parts = 4, writer_threads = 4, device = 0;
+    // lookahead; empty / negative = from the sidecar JSON, else the default
+    std::string la_path, la_mode;
+    double la_beta = -1.0;
+    int la_every = -1, la_hidden = -1, la_layers = -1;
 };
+
+std::string slurp(const std::string &path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return std::string();
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+// A one-dimensional little-endian float32 .npy array (format versions 1-3).
+bool read_npy_f32(const std::string &path, std::vector<float> &out) {
+    const std::string b = slurp(path);
+    if (b.size() < 10 || b.compare(0, 6, "\x93NUMPY") != 0) return false;
+    const int major = (unsigned char)b[6];
+    size_t hlen, h0;
+    if (major == 1) {
+        hlen = (unsigned char)b[8] | ((size_t)(unsigned char)b[9] << 8);
+        h0 = 10;
+    } else {
+        if (b.size() < 12) return false;
+        hlen = 0;
+        for (int k = 0; k < 4; k++) hlen |= (size_t)(unsigned char)b[8 + k] << (8 * k);
+        h0 = 12;
+    }
+    if (h0 + hlen > b.size()) return false;
+    const std::string h = b.substr(h0, hlen);
+    if (h.find("'descr': '<f4'") == std::string::npos || h.find("'fortran_order': False") == std::string::npos)
+        return false;
+    const size_t sp = h.find("'shape': (");
+    if (sp == std::string::npos) return false;
+    const size_t close = h.find(')', sp);
+    if (close == std::string::npos) return false;
+    const std::string dims = h.substr(sp + 10, close - sp - 10);  // "n," for one dimension
+    if (dims.empty() || dims.back() != ',' || dims.find(',') != dims.size() - 1) return false;
+    const long long n = atoll(dims.c_str());
+    if (n < 0) return false;
+    if (h0 + hlen + (size_t)n * 4 != b.size()) return false;
+    out.resize((size_t)n);
+    memcpy(out.data(), b.data() + h0 + hlen, (size_t)n * 4);
+    return true;
+}
+
+// The value of the first "key": in a flat settings file (numbers or strings).
+std::string json_value(const std::string &doc, const char *key) {
+    const std::string k = std::string("\"") + key + "\":";
+    size_t p = doc.find(k);
+    if (p == std::string::npos) return std::string();
+    p += k.size();
+    while (p < doc.size() && (doc[p] == ' ' || doc[p] == '\n')) p++;
+    if (p < doc.size() && doc[p] == '"') {
+        const size_t e = doc.find('"', p + 1);
+        return e == std::string::npos ? std::string() : doc.substr(p + 1, e - p - 1);
+    }
+    size_t e = p;
+    while (e < doc.size() && (isdigit((unsigned char)doc[e]) || doc[e] == '.' || doc[e] == '-' || doc[e] == 'e' ||
+                              doc[e] == 'E' || doc[e] == '+'))
+        e++;
+    return doc.substr(p, e - p);
+}
 
 double now() {
     using namespace std::chrono;
@@ -79,10 +150,19 @@ int main(int argc, char **argv) {
             val(t);
         } else if (s == "-device") ival(a.device);
         else if (s == "-graph") a.graph = true;
+        else if (s == "-lookahead") val(a.la_path);
+        else if (s == "-la_mode") val(a.la_mode);
+        else if (s == "-la_beta") {
+            if (i + 1 < argc) a.la_beta = atof(argv[++i]);
+        } else if (s == "-la_every") ival(a.la_every);
+        else if (s == "-la_hidden") ival(a.la_hidden);
+        else if (s == "-la_layers") ival(a.la_layers);
     }
     if (a.cap.empty() || a.net.empty() || a.out.empty()) {
         fprintf(stderr, "usage: route -cap F -net F -gr_out F [-new_fmt] -bit_pmodel -batch_part "
-                        "[-num_xdim_parts k] [-wrt_mrg] [-rseg_fmt] [-oprd_ppatch] [-graph] [-report F]\n");
+                        "[-num_xdim_parts k] [-wrt_mrg] [-rseg_fmt] [-oprd_ppatch] [-graph] [-report F] "
+                        "[-lookahead F.npy [-la_mode demand|excess] [-la_beta b] [-la_every k] [-la_hidden h] "
+                        "[-la_layers l]]\n");
         return 2;
     }
     if (!a.bit_pmodel || a.rbt || a.ord || a.upd24) {
@@ -90,6 +170,32 @@ int main(int argc, char **argv) {
         return 2;
     }
     if (a.parts < 1) a.parts = 1;
+
+    std::vector<float> la_params;
+    if (!a.la_path.empty()) {
+        if (!read_npy_f32(a.la_path, la_params)) {
+            fprintf(stderr, "route: %s is not a one-dimensional float32 .npy file\n", a.la_path.c_str());
+            return 2;
+        }
+        std::string side = a.la_path;
+        if (side.size() > 4 && side.compare(side.size() - 4, 4, ".npy") == 0) side.resize(side.size() - 4);
+        const std::string js = slurp(side + ".json");
+        auto num = [&](const char *key, double dflt) {
+            const std::string v = json_value(js, key);
+            return v.empty() ? dflt : atof(v.c_str());
+        };
+        if (a.la_mode.empty()) a.la_mode = json_value(js, "mode");
+        if (a.la_mode.empty()) a.la_mode = "demand";
+        if (a.la_beta < 0) a.la_beta = num("beta", 0.5);
+        if (a.la_every < 0) a.la_every = (int)num("every", 16);
+        if (a.la_hidden < 0) a.la_hidden = (int)num("hidden", 32);
+        if (a.la_layers < 0) a.la_layers = (int)num("layers", 4);
+        if ((a.la_mode != "demand" && a.la_mode != "excess") || a.la_every < 1 || a.la_hidden < 1 ||
+            a.la_layers < 2) {
+            fprintf(stderr, "route: bad lookahead settings\n");
+            return 2;
+        }
+    }
 
     const double t0 = now();
     gr_design *d = nullptr;
@@ -121,12 +227,30 @@ int main(int argc, char **argv) {
     const int64_t slots = gr_plan_slots(ctx);
     std::vector<int64_t> mst(slots > 0 ? slots : 1);
     std::vector<int32_t> pat(slots > 0 ? slots : 1);
+    gr_cnn *cnn = nullptr;
+    if (!a.la_path.empty()) {
+        if ((rc = gr_cnn_create(&cnn, a.device, 2 * Z, Z, a.la_hidden, a.la_layers, Y, X, 1)))
+            return fail("creating the lookahead network", rc);
+        if (gr_cnn_num_params(cnn) != (int64_t)la_params.size()) {
+            fprintf(stderr, "route: %s holds %zu parameters, a %d-layer network of %d channels on Z=%d needs %lld\n",
+                    a.la_path.c_str(), la_params.size(), a.la_layers, a.la_hidden, Z,
+                    (long long)gr_cnn_num_params(cnn));
+            return 2;
+        }
+        if ((rc = gr_cnn_set_params(cnn, la_params.data()))) return fail("loading the lookahead network", rc);
+    }
     if ((rc = gr_sync(ctx))) return fail("setup", rc);
     const double t3 = now();
-    rc = gr_route_design_host(ctx, n_nets, pin_ofs.data(), pins.data(), n_batches, bofs.data(), ids.data(),
-                              mst.data(), pat.data(), a.graph ? GR_PLAN_GRAPH : 0);
+    if (cnn)
+        rc = gr_route_design_lookahead_host(ctx, cnn, a.la_every, (float)a.la_beta,
+                                            a.la_mode == "excess" ? GR_LA_EXCESS : GR_LA_DEMAND, mst.data(),
+                                            pat.data());
+    else
+        rc = gr_route_design_host(ctx, n_nets, pin_ofs.data(), pins.data(), n_batches, bofs.data(), ids.data(),
+                                  mst.data(), pat.data(), a.graph ? GR_PLAN_GRAPH : 0);
     if (rc) return fail("routing", rc);
     const double t4 = now();
+    if (cnn) printf("route: lookahead %s, beta %g, every %d batches\n", a.la_mode.c_str(), a.la_beta, a.la_every);
 
     int64_t wv[2] = {0, 0};
     const int flags = (a.wrt_mrg ? GR_WRT_MERGE : 0) | (a.rseg ? GR_WRT_RSEG : 0) | (a.ppatch ? GR_WRT_PPATCH : 0);
@@ -157,6 +281,7 @@ int main(int argc, char **argv) {
             fclose(f);
         }
     }
+    if (cnn) gr_cnn_destroy(cnn);
     gr_destroy(ctx);
     gr_design_free(d);
     return 0;

@@ -16,6 +16,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _capi
 from ._capi import (GR_PLAN_GRAPH, GR_WRT_MERGE, GR_WRT_PPATCH, GR_WRT_RSEG, check, i32, i64, lib, ptr)
 
 
@@ -206,6 +207,15 @@ class Router:
         check(self._lib.gr_route_design_host(self._h, len(pin_ofs) - 1, ptr(pin_ofs), ptr(pins),
                                              len(batch_ofs) - 1, ptr(batch_ofs), ptr(net_ids), ptr(mst_out),
                                              ptr(pat_out), 0), "gr_route_design_host")
+
+    def route_lookahead_host(self, net, every: int, beta: float, mode: str, mst_out, pat_out=None):
+        """The uploaded plan routed from reset with the lookahead cost, all in
+        the library (gr_route_design_lookahead_host); results into host
+        numpy arrays of plan_slots entries."""
+        modes = {"demand": _capi.GR_LA_DEMAND, "excess": _capi.GR_LA_EXCESS}
+        check(self._lib.gr_route_design_lookahead_host(self._h, net._h, every, C.c_float(beta), modes[mode],
+                                                       ptr(mst_out), ptr(pat_out) if pat_out is not None else None),
+              "gr_route_design_lookahead_host")
 
     # ---------------------------------------------------------- lookahead
     def features(self, scale: float = 1.0 / 16):

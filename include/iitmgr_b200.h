@@ -189,6 +189,19 @@ int64_t gr_launch_count(gr_ctx *ctx);
 int gr_features(gr_ctx *ctx, float *d_feat, float scale, void *stream);
 int gr_set_lookahead(gr_ctx *ctx, const float *d_pred, float beta, void *stream);
 
+/* The whole lookahead route of the uploaded plan (gr_plan_set) from reset:
+ * before every `every` batches the network (gr_cnn, 2Z inputs and Z outputs
+ * over the Y x X grid) predicts from the current state (features x 1/16) the
+ * further demand (output x 16), in GR_LA_EXCESS mode only its part beyond
+ * the remaining capacity, and gr_set_lookahead(prediction, beta) applies
+ * it. MST slots and patterns are copied to host memory; the plain cost is
+ * restored at the end. beta == 0 routes plainly. */
+#define GR_LA_DEMAND 0
+#define GR_LA_EXCESS 1
+typedef struct gr_cnn gr_cnn;
+int gr_route_design_lookahead_host(gr_ctx *ctx, gr_cnn *cnn, int32_t every, float beta, int mode,
+                                   int64_t *h_mst_edges, int32_t *h_mst_pat);
+
 /* Launch shapes of the Boruvka size classes (results do not depend on them;
  * the autotuner in iitmglobalrouter_b200/tune.py picks them per GPU and Z). */
 #define GR_TUNE_MST_MID_THREADS 0      /* threads per CTA, nets of 33..128 pins  */
@@ -258,12 +271,14 @@ int gr_design_eval(const gr_design *d, const int32_t *demand, double *out3);
  * the demand still to come, predicted from the current demand and capacity.
  * BF16 tensor-core GEMMs with FP32 accumulation, FP32 master parameters
  * (per layer: weights [cout][cin][3][3], then biases), Adam updates on a
- * mean-squared-error loss. d_* are device pointers; calls synchronise. */
-typedef struct gr_cnn gr_cnn;
+ * mean-squared-error loss. d_* are device pointers; calls synchronise.
+ * (gr_cnn is declared above, beside gr_route_design_lookahead_host.) */
 int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, int hidden, int n_layers, int H,
                   int W, uint64_t seed);
 int gr_cnn_destroy(gr_cnn *cnn);
 int64_t gr_cnn_num_params(gr_cnn *cnn);
+/* the CUDA device, input and output channels and grid of a network */
+int gr_cnn_info(gr_cnn *cnn, int *device, int *in_channels, int *out_channels, int *H, int *W);
 int gr_cnn_get_params(gr_cnn *cnn, float *h_out);
 int gr_cnn_set_params(gr_cnn *cnn, const float *h_in);
 int gr_cnn_forward(gr_cnn *cnn, const float *d_in, float *d_out);

@@ -47,3 +47,22 @@ def test_route_cli_rejects_other_modes(tmp_path):
     cmd = [str(gr.LIB_PATH.parent / "route"), "-cap", "x", "-net", "y", "-gr_out", "z", "-rbt_part"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=60)
     assert r.returncode == 2
+
+
+def test_route_cli_rejects_bad_lookahead_files(tmp_path):
+    """A network file that is not a one-dimensional float32 .npy, or settings
+    out of range, stop the tool before any device work (runs without a GPU)."""
+    import numpy as np
+
+    route = str(gr.LIB_PATH.parent / "route")
+    base = [route, "-cap", "x", "-net", "y", "-gr_out", "z", "-bit_pmodel", "-batch_part", "-lookahead"]
+    np.save(tmp_path / "two_d.npy", np.zeros((3, 4), np.float32))
+    np.save(tmp_path / "f64.npy", np.zeros(5, np.float64))
+    (tmp_path / "junk.npy").write_bytes(b"not a numpy file")
+    for name in ("two_d.npy", "f64.npy", "junk.npy", "missing.npy"):
+        r = subprocess.run(base + [str(tmp_path / name)], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2 and "float32 .npy" in r.stderr, (name, r.stderr)
+    np.save(tmp_path / "ok.npy", np.zeros(5, np.float32))
+    for extra in (["-la_mode", "sideways"], ["-la_every", "0"], ["-la_layers", "1"]):
+        r = subprocess.run(base + [str(tmp_path / "ok.npy")] + extra, capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2 and "bad lookahead settings" in r.stderr, (extra, r.stderr)

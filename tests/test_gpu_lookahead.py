@@ -123,3 +123,106 @@ def test_trained_network_lowers_overflow(cuda):
     plain, la = res[0.0], res[0.5]
     assert la["overflow"] < plain["overflow"]
     assert la["wirelength"] <= 1.01 * plain["wirelength"]
+
+
+def _strong_net(R, Z, seed=5):
+    """A random network scaled until its predicted excess over the remaining
+    capacity is positive on a few per cent of the cells of the empty grid
+    (so both modes change the route)."""
+    import torch
+
+    net = lookahead.LookaheadNet(2 * Z, Z, R.Y, R.X, hidden=8, n_layers=3, seed=seed)
+    p = net.get_params()
+    R.reset()
+    f = R.features(lookahead.SCALE)
+    for _ in range(12):
+        pred = net.forward(f) * (1.0 / lookahead.SCALE)
+        if float((torch.relu(pred - (f[Z:] - f[:Z]) * (1.0 / lookahead.SCALE)) > 0).float().mean()) > 0.03:
+            break
+        p = p * 2.0
+        net.set_params(p)
+    return net
+
+
+@pytest.mark.parametrize("mode,beta,every", [("demand", 1.0, 3), ("excess", 0.5, 2), ("excess", 0.0, 4)])
+def test_lookahead_host_entry_matches_python_driver(cuda, mode, beta, every):
+    """gr_route_design_lookahead_host (network, prediction transform, cost
+    switch and routing all inside the library) gives exactly the trees,
+    patterns, demand and Fenwick trees of the Python driver; beta 0 is the
+    plain route of the oracle."""
+    d, R, mst, pat, ofs, pins, bofs, ids = _setup(1, seed=3)
+    nb = len(bofs) - 1
+    net = _strong_net(R, R.Z)
+    lookahead.route_lookahead(R, net, mst, pat, nb, every=every, beta=beta, mode=mode)
+    want = (mst.cpu().numpy(), pat.cpu().numpy(), R.demand(), R.fenwick().view(np.uint32))
+    R.reset()
+    R.route_plan(mst, pat)
+    R.sync()
+    plain = (mst.cpu().numpy(), pat.cpu().numpy())
+    mst_h = np.full(R.plan_slots, -3, np.int64)
+    pat_h = np.full(R.plan_slots, -3, np.int32)
+    R.route_lookahead_host(net, every, beta, mode, mst_h, pat_h)
+    assert np.array_equal(mst_h, want[0]) and np.array_equal(pat_h, want[1])
+    assert np.array_equal(R.demand(), want[2])
+    assert np.array_equal(R.fenwick().view(np.uint32), want[3])
+    if beta > 0:
+        assert not (np.array_equal(mst_h, plain[0]) and np.array_equal(pat_h, plain[1]))  # the lookahead acted
+    else:
+        g = oracle.Grid(R.X, R.Y, R.Z, d.caps())
+        rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=8)
+        assert rc == 0 and np.array_equal(mst_h, mst_c) and np.array_equal(pat_h, mp_c)
+
+
+def test_lookahead_host_entry_rejects_mismatched_network(cuda):
+    import ctypes as C
+
+    from iitmglobalrouter_b200 import _capi
+
+    d, R, *_ = _setup(1, seed=3)
+    net = lookahead.LookaheadNet(2 * R.Z, R.Z, R.Y, R.X + 1, hidden=8, n_layers=2)
+    out = np.zeros(R.plan_slots, np.int64)
+    L = gr.lib()
+    rc = L.gr_route_design_lookahead_host(R._h, net._h, 4, C.c_float(1.0), 0, out.ctypes.data_as(C.c_void_p), None)
+    assert rc == -1, _capi.ERRORS.get(rc, rc)
+    net = lookahead.LookaheadNet(2 * R.Z, R.Z, R.Y, R.X, hidden=8, n_layers=2)
+    for every, beta, mode in ((0, 1.0, 0), (4, -1.0, 0), (4, 1.0, 2)):
+        rc = L.gr_route_design_lookahead_host(R._h, net._h, every, C.c_float(beta), mode,
+                                              out.ctypes.data_as(C.c_void_p), None)
+        assert rc == -1
+
+
+@pytest.mark.parametrize("mode", ["demand", "excess"])
+def test_route_cli_lookahead_matches_python_driver(cuda, tmp_path, mode):
+    """`route -lookahead F.npy` (settings from F.json) writes the route file
+    that the Python driver's trees and patterns give."""
+    import json
+    import subprocess
+
+    import torch
+
+    d = gr.Design.generate(1, seed=4)
+    cap, net_f, out = tmp_path / "d.cap", tmp_path / "d.net", tmp_path / "d.route"
+    d.write(cap, net_f)
+    rd = gr.Design.read(cap, net_f)
+    dims = rd.dims
+    ofs, pins = rd.nets()
+    bofs, ids = rd.batch(4)
+    R = gr.Router(dims["X"], dims["Y"], dims["Z"], rd.caps())
+    R.set_nets(ofs, pins)
+    R.plan_set(bofs, ids)
+    net = _strong_net(R, R.Z, seed=9)
+    np.save(tmp_path / "w.npy", net.get_params().astype(np.float32))
+    beta, every = (0.75, 2) if mode == "demand" else (0.5, 3)
+    (tmp_path / "w.json").write_text(json.dumps({"hidden": 8, "layers": 3, "every": every, "beta": beta,
+                                                 "mode": mode}))
+    mst = torch.empty(R.plan_slots, dtype=torch.int64, device="cuda")
+    pat = torch.empty(R.plan_slots, dtype=torch.int32, device="cuda")
+    lookahead.route_lookahead(R, net, mst, pat, len(bofs) - 1, every=every, beta=beta, mode=mode)
+    ref = tmp_path / "py.route"
+    rd.write_routes(ref, mst.cpu().numpy(), pat.cpu().numpy(), merge=True, rseg=False, ppatch=False)
+    cmd = [str(gr.LIB_PATH.parent / "route"), "-cap", str(cap), "-net", str(net_f), "-gr_out", str(out), "-new_fmt",
+           "-bit_pmodel", "-batch_part", "-num_xdim_parts", "4", "-wrt_mrg", "-lookahead", str(tmp_path / "w.npy")]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert f"lookahead {mode}" in r.stdout
+    assert out.read_bytes() == ref.read_bytes()
