@@ -108,6 +108,195 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
         }
 }
 
+// ------------------------------------------------------------------ forward convolution on tcgen05
+// One CTA computes 128 positions x Nt (16 or 32) output channels of a layer
+// as an implicit GEMM: the 128 x Kp patch matrix is gathered from the input
+// (fp32 -> bf16, zero outside the grid) straight into shared memory in the
+// canonical K-major layout without swizzle (8-row x 16-byte core matrices;
+// core matrix (row group g, k chunk c) at c * LBO + g * 128 bytes), the
+// weights likewise as an Nt x Kp matrix; one thread issues the Kp / 16
+// tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator of 128 lanes x Nt
+// columns in tensor memory) and commits them to an mbarrier; the epilogue
+// reads the accumulator with tcgen05.ld (warp w: lanes 32 (w % 4) .., columns
+// 16 (w / 4) ..), adds the bias, applies ReLU and writes Y[n][m] (coalesced
+// over m) and, when training, the pre-activation Z[m][n].
+constexpr int kConvThreads = 256, kConvRows = 128, kConvTmemCols = 32;
+constexpr int kConvSmemMax = 200 * 1024;
+constexpr long long kConvWaitLimit = 1ll << 24;  // mbarrier polls before the kernel reports a stall
+
+__host__ __device__ constexpr int conv_smem_bytes(int Kp, int Nt) {
+    return 1024 + kConvRows * Kp * 2 + Nt * Kp * 2 + 64;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start, leading (k chunk) and stride (row
+// group) byte offsets in 16-byte units, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kConvWaitLimit; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+__global__ void __launch_bounds__(kConvThreads, 2)
+    k_conv_tc(int cin, int cout, int H, int W, int Kp, int Nt, int Np, const float *__restrict__ X,
+              const __nv_bfloat16 *__restrict__ Wt, const float *__restrict__ bias, float *__restrict__ Y,
+              float *__restrict__ Zp, int relu, int *__restrict__ err) {
+    extern __shared__ uint8_t conv_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)conv_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *As = base;                                   // 128 x Kp
+    uint8_t *Bs = As + kConvRows * Kp * 2;                // Nt x Kp
+    uint64_t *bar = (uint64_t *)(Bs + Nt * Kp * 2);       // 8-byte aligned (Kp multiple of 16)
+    uint32_t *tmem_slot = (uint32_t *)(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = H * W, m0 = blockIdx.x * kConvRows;
+    const int nchunk = Kp >> 3;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kConvTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 32) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+
+    // weights: B(n, k) = Wt[k][n] for n < Np, zero beyond
+    for (int i = tid; i < Nt * nchunk; i += kConvThreads) {
+        const int n = i % Nt, c = i / Nt;
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int k = 8 * c + 2 * j;
+            const __nv_bfloat16 z = __float2bfloat16(0.0f);
+            const __nv_bfloat16 lo = n < Np ? Wt[(long long)k * Np + n] : z;
+            const __nv_bfloat16 hi = n < Np ? Wt[(long long)(k + 1) * Np + n] : z;
+            w[j] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+        }
+        *(uint4 *)(Bs + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+
+    // patches: thread (row r, half h) fills k chunks [h * nchunk / 2, (h + 1) * nchunk / 2) of row r
+    {
+        const int r = tid & (kConvRows - 1), h = tid >> 7;
+        const int m = m0 + r;
+        const int c0 = h * (nchunk >> 1), c1 = h ? nchunk : (nchunk >> 1);  // nchunk is even (Kp % 16 == 0)
+        const int y = m < M ? m / W : 0, x = m < M ? m - y * W : 0;
+        int vmask = 0;  // bit dy * 3 + dx: tap inside the grid
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+            vmask |= (m < M && yy >= 0 && yy < H && xx >= 0 && xx < W) << t;
+        }
+        int ci = (8 * c0) / 9, tap = 8 * c0 - 9 * ci;
+        for (int c = c0; c < c1; c++) {
+            uint32_t w[4];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                float v = 0.0f;
+                if (ci < cin && ((vmask >> tap) & 1)) {
+                    const int dy = tap / 3, dx = tap - 3 * dy;
+                    v = __ldg(X + (long long)ci * M + m + (dy - 1) * W + (dx - 1));
+                }
+                const uint32_t b = __bfloat16_as_ushort(__float2bfloat16(v));
+                if (j & 1) w[j >> 1] |= b << 16;
+                else w[j >> 1] = b;
+                if (++tap == 9) tap = 0, ci++;
+            }
+            *(uint4 *)(As + (size_t)c * (kConvRows * 16) + r * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0) {
+        const uint32_t idesc = umma_idesc_bf16(kConvRows, Nt);
+        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
+        const uint32_t a_lbo = kConvRows * 16, b_lbo = Nt * 16;
+        for (int s = 0; s < (Kp >> 4); s++) {
+            const uint64_t ad = umma_sdesc(a0 + 2 * s * a_lbo, a_lbo, 128);
+            const uint64_t bd = umma_sdesc(b0 + 2 * s * b_lbo, b_lbo, 128);
+            const uint32_t acc = s > 0;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         smem_u32(bar))
+                     : "memory");
+    }
+    const bool done = mbar_wait_bounded(smem_u32(bar), 0);
+    if (!done && lane == 0) atomicOr(err, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    const int q = warp & 3, half = warp >> 2;
+    if (done && 16 * half < Nt) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * half, v);
+        const int m = m0 + 32 * q + lane;
+        if (m < M) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const int n = 16 * half + j;
+                if (n < cout) {
+                    const float o = v[j] + bias[n];
+                    Y[(long long)n * M + m] = relu ? fmaxf(o, 0.0f) : o;
+                    if (Zp) Zp[(long long)m * Np + n] = v[j];
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kConvTmemCols)
+                     : "memory");
+    }
+}
+
 // ------------------------------------------------------------------ layer pieces
 __global__ void k_im2col(int Cin, int H, int W, int Kp, const float *__restrict__ X, __nv_bfloat16 *__restrict__ col) {
     const long long total = (long long)H * W * Kp;
@@ -255,6 +444,7 @@ struct gr_cnn {
     __nv_bfloat16 *col = nullptr, *dz = nullptr;
     float *dcol = nullptr, *dact = nullptr, *dact2 = nullptr, *loss = nullptr;
     int64_t adam_t = 0;
+    int *err = nullptr;  // device: set by a convolution whose accumulator wait gave up
     cudaStream_t stream = nullptr;
 };
 
@@ -278,15 +468,32 @@ int pack_all(gr_cnn *c) {
     return GR_OK;
 }
 
-int forward(gr_cnn *c) {
+// the tensor-core convolution takes a layer whose tiles fit in shared memory
+bool conv_tc_fits(const gr_cnn *c, int l) {
+    return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16)) <= kConvSmemMax;
+}
+
+int forward(gr_cnn *c, bool keep_z) {
     const int M = c->H * c->W;
     cudaStream_t s = c->stream;
+    static bool attr_set = false;  // the attribute holds for the process; one constant value
+    if (!attr_set) {
+        CN_CK(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
+        attr_set = true;
+    }
     for (int l = 0; l < c->n_layers; l++) {
+        const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
+        if (conv_tc_fits(c, l)) {
+            const int Nt = round_up(c->cout[l], 16);
+            k_conv_tc<<<(M + kConvRows - 1) / kConvRows, kConvThreads, conv_smem_bytes(c->Kp[l], Nt), s>>>(
+                c->cin[l], c->cout[l], c->H, c->W, c->Kp[l], Nt, c->Np[l], c->act[l], c->wt[l], bl, c->act[l + 1],
+                keep_z ? c->z[l] : nullptr, l + 1 < c->n_layers, c->err);
+            continue;
+        }
         k_im2col<<<grid((long long)M * c->Kp[l]), 256, 0, s>>>(c->cin[l], c->H, c->W, c->Kp[l], c->act[l], c->col);
         int rc = gemm(s, M, c->Np[l], c->Kp[l], c->col, c->Kp[l], 1, c->wt[l], c->Np[l], 1, c->z[l], c->Np[l], 1, 1);
         if (rc) return rc;
-        const float *b = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
-        k_bias_act<<<grid((long long)M * c->cout[l]), 256, 0, s>>>(M, c->cout[l], c->Np[l], c->z[l], b,
+        k_bias_act<<<grid((long long)M * c->cout[l]), 256, 0, s>>>(M, c->cout[l], c->Np[l], c->z[l], bl,
                                                                    c->act[l + 1], l + 1 < c->n_layers);
     }
     CN_CK(cudaGetLastError());
@@ -323,6 +530,19 @@ int backward(gr_cnn *c, const float *d_target) {
         }
     }
     CN_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+// waits for the network's stream; a convolution that gave up waiting for its
+// accumulator is reported (and the flag cleared)
+int finish(gr_cnn *c) {
+    int err = 0;
+    CN_CK(cudaMemcpyAsync(&err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CN_CK(cudaStreamSynchronize(c->stream));
+    if (err) {
+        CN_CK(cudaMemset(c->err, 0, sizeof(int)));
+        return GR_ERR_DEVICE;
+    }
     return GR_OK;
 }
 
@@ -372,6 +592,7 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
     ok = ok && cudaMalloc(&c->dact, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->dact2, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->loss, sizeof(float) * 2) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->err, sizeof(int)) == cudaSuccess && cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
     for (int l = 0; l <= n_layers && ok; l++)
         ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
     for (int l = 0; l < n_layers && ok; l++) {
@@ -410,7 +631,7 @@ int gr_cnn_destroy(gr_cnn *c) {
     if (!c) return GR_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void *p : {(void *)c->params, (void *)c->grads, (void *)c->m1, (void *)c->m2, (void *)c->col, (void *)c->dz,
-                    (void *)c->dcol, (void *)c->dact, (void *)c->dact2, (void *)c->loss})
+                    (void *)c->dcol, (void *)c->dact, (void *)c->dact2, (void *)c->loss, (void *)c->err})
         cudaFree(p);
     for (int l = 0; l < kMaxLayers; l++) {
         cudaFree(c->wt[l]);
@@ -456,33 +677,31 @@ int gr_cnn_forward(gr_cnn *c, const float *d_in, float *d_out) {
     if (!c || !d_in || !d_out) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, false);
     if (rc) return rc;
     CN_CK(cudaMemcpyAsync(d_out, c->act[c->n_layers], sizeof(float) * M * c->cout[c->n_layers - 1],
                           cudaMemcpyDeviceToDevice, c->stream));
-    CN_CK(cudaStreamSynchronize(c->stream));
-    return GR_OK;
+    return finish(c);
 }
 
 int gr_cnn_grads(gr_cnn *c, const float *d_in, const float *d_target, float *h_grads, float *h_loss) {
     if (!c || !d_in || !d_target) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, true);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     if (h_grads)
         CN_CK(cudaMemcpyAsync(h_grads, c->grads, sizeof(float) * c->n_params, cudaMemcpyDeviceToHost, c->stream));
     if (h_loss) CN_CK(cudaMemcpyAsync(h_loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-    CN_CK(cudaStreamSynchronize(c->stream));
-    return GR_OK;
+    return finish(c);
 }
 
 int gr_cnn_train_step(gr_cnn *c, const float *d_in, const float *d_target, float lr, float *h_loss) {
     if (!c || !d_in || !d_target || !(lr > 0.0f)) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, true);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     c->adam_t++;
@@ -495,8 +714,7 @@ int gr_cnn_train_step(gr_cnn *c, const float *d_in, const float *d_target, float
     rc = pack_all(c);
     if (rc) return rc;
     if (h_loss) CN_CK(cudaMemcpyAsync(h_loss, c->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-    CN_CK(cudaStreamSynchronize(c->stream));
-    return GR_OK;
+    return finish(c);
 }
 
 // test hook: one GEMM C = A * B of row-major bf16 matrices (A: M x K, B: K x N),

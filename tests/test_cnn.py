@@ -59,11 +59,61 @@ def _net_case(seed=3, H=12, W=10, cin=4, cout=2, hidden=8, layers=3):
     return net, x, t
 
 
+def _bf16_round(a):
+    """float32 -> nearest bfloat16 (ties to even), returned as float32."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
 @pytest.mark.gpu
-def test_forward_matches_reference(cuda):
+@pytest.mark.parametrize("H,W,cin,hidden,cout", [
+    (37, 29, 20, 32, 20),  # 9 tiles of 128 positions, the last ragged; Kp 192; 32 output columns
+    (16, 8, 32, 16, 10),  # exactly one tile; Kp 288; 16 output columns
+    (50, 50, 32, 32, 32),  # 20 tiles
+])
+def test_forward_exact_on_binary_grid(cuda, H, W, cin, hidden, cout):
+    """Inputs on multiples of 1/16 in [0, 4) and weights on multiples of 1/64
+    in [-1, 1]: every first-layer sum is exact in FP32 whatever the order of
+    accumulation, and the second layer copies channel j of the (BF16-rounded)
+    ReLU output to output j through its centre tap. The forward must then equal
+    the float64 value bit for bit -- gather, shared-memory layout, tensor-core
+    tiles, bias, ReLU and the ragged last tile all checked exactly."""
     import torch
 
-    net, x, _ = _net_case()
+    from iitmglobalrouter_b200.lookahead import LookaheadNet
+
+    rng = np.random.default_rng(H * W + cin)
+    net = LookaheadNet(cin, cout, H, W, hidden=hidden, n_layers=2, seed=1)
+    w1 = rng.integers(-64, 65, size=(hidden, cin, 3, 3)) / 64.0
+    b1 = rng.integers(-64, 65, size=hidden) / 64.0
+    w2 = np.zeros((cout, hidden, 3, 3))
+    for j in range(cout):
+        w2[j, j, 1, 1] = 1.0
+    p = np.concatenate([w1.ravel(), b1, w2.ravel(), np.zeros(cout)]).astype(np.float32)
+    assert p.size == net.num_params
+    net.set_params(p)
+    x = (rng.integers(0, 64, size=(cin, H, W)) / 16.0).astype(np.float32)
+    y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    xp = np.pad(x.astype(np.float64), ((0, 0), (1, 1), (1, 1)))
+    z = np.zeros((hidden, H, W))
+    for dy in range(3):
+        for dx in range(3):
+            z += np.einsum("oc,chw->ohw", w1[:, :, dy, dx], xp[:, dy:dy + H, dx:dx + W])
+    z += b1[:, None, None]
+    want = _bf16_round(np.maximum(z, 0.0).astype(np.float32))[:cout]
+    assert np.array_equal(y.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [
+    dict(),  # one partial tile of 128 positions
+    dict(H=9, W=40, cin=80, cout=3, hidden=16, layers=2),  # first layer too wide for the tensor-core tile: GEMM path
+])
+def test_forward_matches_reference(cuda, shape):
+    import torch
+
+    net, x, _ = _net_case(**shape)
     p = net.get_params()
     p[-net.out_channels:] = 0.25  # a nonzero bias somewhere
     net.set_params(p)
