@@ -6,11 +6,13 @@
 //   forward   col[m][k] = X[ci][y+dy][x+dx]          (im2col, k = ci*9 + (dy+1)*3 + dx+1, m = y*W + x)
 //             Z[m][n]   = sum_k col[m][k] * Wt[k][n] (GEMM, mma.sync m16n8k16 bf16 -> f32)
 //             Y[n][m]   = act(Z[m][n] + b[n])         (ReLU on every layer but the last)
-//   backward  dZ = dY * act'(Z)
-//             dWt[k][n] = sum_m col[m][k] dZ[m][n]    (GEMM over the positions, split across blocks)
-//             db[n]     = sum_m dZ[m][n]
-//             dcol[m][k]= sum_n dZ[m][n] Wt[k][n]      (GEMM)
-//             dX        = col2im(dcol)                 (each input gathers its nine taps)
+//   backward  dZ = dY * act'(Z)                     (ReLU mask from the layer's output)
+//             dW[n][k]  = sum_m col[m][k] dZ[n][m],   db[n] = sum_m dZ[n][m]
+//                         (one tensor-core GEMM over the positions with the patches
+//                          gathered on the fly and a row of ones for the bias)
+//             dX[ci]    = sum over co, taps of dZ[co] shifted * W[co][ci] flipped
+//                         (a 3x3 convolution of dZ with the weights transposed and
+//                          rotated by 180 degrees: the forward convolution kernel)
 // The loss is the mean squared error of the last layer against the target;
 // parameters are FP32 masters updated by Adam, cast to BF16 for the GEMMs.
 #include <cuda_bf16.h>
@@ -297,6 +299,156 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     }
 }
 
+// ------------------------------------------------------------------ weight gradient on tcgen05
+// D[r][n] = sum over positions p of A[r][p] * B[n][p] for the 128 rows r of
+// tile blockIdx.y, over the position range of blockIdx.x:
+//   A[r][p] = X[ci][p + offset of tap t] (r = ci * 9 + t < 9 cin; zero outside the grid)
+//             1 for r == 9 cin (the bias row), 0 beyond
+//   B[n][p] = dZ[n][p] (channel-major fp32, already masked by the ReLU derivative)
+// Stages of 64 positions (four K = 16 MMAs) are gathered into one of two
+// shared-memory buffers while the tensor core consumes the other; each
+// buffer's MMAs are committed to its own mbarrier. The 128 x Nt partial sums
+// are added (atomics) into the gradient in parameter layout: g[n][r] for the
+// weights, g[cout * 9 cin + n] for the bias.
+constexpr int kWgPos = 64;
+
+__host__ __device__ constexpr int wgrad_smem_bytes(int Nt) {
+    return 1024 + 2 * (kConvRows * kWgPos * 2) + 2 * (Nt * kWgPos * 2) + 64;
+}
+
+__global__ void __launch_bounds__(kConvThreads, 2)
+    k_wgrad_tc(int cin, int cout, int H, int W, int Nt, int per_split, const float *__restrict__ X,
+               const float *__restrict__ dZ, float *__restrict__ g, int *__restrict__ err) {
+    extern __shared__ uint8_t wg_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)wg_raw + 1023) & ~(uintptr_t)1023);
+    constexpr int a_bytes = kConvRows * kWgPos * 2;
+    const int b_bytes = Nt * kWgPos * 2;
+    uint8_t *As0 = base, *Bs0 = base + 2 * a_bytes;                // buffer b at + b * a_bytes / b * b_bytes
+    uint64_t *bar = (uint64_t *)(Bs0 + 2 * b_bytes);              // two barriers
+    uint32_t *tmem_slot = (uint32_t *)(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = H * W, K9 = 9 * cin, r0 = blockIdx.y * kConvRows;
+    const int p0 = blockIdx.x * per_split, p1 = min(M, p0 + per_split);
+    const int nst = p1 > p0 ? (p1 - p0 + kWgPos - 1) / kWgPos : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kConvTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 32) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar + 1)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = umma_idesc_bf16(kConvRows, Nt);
+
+    bool ok = true;
+    for (int st = 0; st < nst && ok; st++) {
+        const int b = st & 1, pb = p0 + st * kWgPos;
+        if (st >= 2) {  // buffer b is free once the MMAs of stage st - 2 are done
+            ok = __syncthreads_and(mbar_wait_bounded(smem_u32(bar + b), ((st - 2) >> 1) & 1));
+            if (!ok) break;
+        }
+        // A: 128 rows x 8 chunks of 8 positions; item i -> row i % 128, chunk i / 128
+        for (int i = tid; i < kConvRows * (kWgPos / 8); i += kConvThreads) {
+            const int rr = i & (kConvRows - 1), ch = i >> 7, r = r0 + rr;
+            const int p = pb + ch * 8;
+            uint32_t w[4] = {0u, 0u, 0u, 0u};
+            if (r < K9) {
+                const int ci = r / 9, t = r - 9 * ci, dy = t / 3 - 1, dx = t - 3 * (t / 3) - 1;
+                int y = p / W, x = p - y * W;
+                const float *Xc = X + (long long)ci * M;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int yy = y + dy, xx = x + dx;
+                    float v = 0.0f;
+                    if (p + j < p1 && yy >= 0 && yy < H && xx >= 0 && xx < W) v = __ldg(Xc + yy * W + xx);
+                    const uint32_t h = __bfloat16_as_ushort(__float2bfloat16(v));
+                    w[j >> 1] |= (j & 1) ? h << 16 : h;
+                    if (++x == W) x = 0, y++;
+                }
+            } else if (r == K9) {
+                const uint32_t one = __bfloat16_as_ushort(__float2bfloat16(1.0f));
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (p + j < p1) w[j >> 1] |= (j & 1) ? one << 16 : one;
+            }
+            *(uint4 *)(As0 + b * a_bytes + ch * (kConvRows * 16) + rr * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        // B: Nt rows x 8 chunks
+        for (int i = tid; i < Nt * (kWgPos / 8); i += kConvThreads) {
+            const int n = i % Nt, ch = i / Nt, p = pb + ch * 8;
+            uint32_t w[4] = {0u, 0u, 0u, 0u};
+            if (n < cout) {
+                const float *dz = dZ + (long long)n * M;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float v = p + j < p1 ? __ldg(dz + p + j) : 0.0f;
+                    const uint32_t h = __bfloat16_as_ushort(__float2bfloat16(v));
+                    w[j >> 1] |= (j & 1) ? h << 16 : h;
+                }
+            }
+            *(uint4 *)(Bs0 + b * b_bytes + ch * (Nt * 16) + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (tid == 0) {
+            const uint32_t a0 = smem_u32(As0 + b * a_bytes), b0 = smem_u32(Bs0 + b * b_bytes);
+            const uint32_t a_lbo = kConvRows * 16, b_lbo = Nt * 16;
+#pragma unroll
+            for (int s = 0; s < kWgPos / 16; s++) {
+                const uint64_t ad = umma_sdesc(a0 + 2 * s * a_lbo, a_lbo, 128);
+                const uint64_t bd = umma_sdesc(b0 + 2 * s * b_lbo, b_lbo, 128);
+                const uint32_t acc = (st > 0 || s > 0);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(bar + b))
+                         : "memory");
+        }
+    }
+    // the last commit of each buffer (the later one covers every MMA issued)
+    if (ok && nst > 1) ok = __syncthreads_and(mbar_wait_bounded(smem_u32(bar + ((nst - 2) & 1)), ((nst - 2) >> 1) & 1));
+    if (ok && nst > 0) ok = __syncthreads_and(mbar_wait_bounded(smem_u32(bar + ((nst - 1) & 1)), ((nst - 1) >> 1) & 1));
+    if (!ok && tid == 0) atomicOr(err, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+    const int q = warp & 3, half = warp >> 2;
+    if (ok && nst > 0 && 16 * half < Nt) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * half, v);
+        const int r = r0 + 32 * q + lane;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int n = 16 * half + j;
+            if (n < cout) {
+                if (r < K9) atomicAdd(g + (long long)n * K9 + r, v[j]);
+                else if (r == K9) atomicAdd(g + (long long)cout * K9 + n, v[j]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kConvTmemCols)
+                     : "memory");
+    }
+}
+
 // ------------------------------------------------------------------ layer pieces
 __global__ void k_im2col(int Cin, int H, int W, int Kp, const float *__restrict__ X, __nv_bfloat16 *__restrict__ col) {
     const long long total = (long long)H * W * Kp;
@@ -327,53 +479,11 @@ __global__ void k_bias_act(int M, int Cout, int Np, const float *__restrict__ Z,
     }
 }
 
-// dZ[m][n] (bf16, padded to Np columns) = dY[n][m] * act'(Z + b)
-__global__ void k_act_grad(int M, int Cout, int Np, const float *__restrict__ dY, const float *__restrict__ Z,
-                           const float *__restrict__ b, __nv_bfloat16 *__restrict__ dZ, int relu) {
-    const long long total = (long long)M * Np;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int n = (int)(i % Np);
-        const long long m = i / Np;
-        float v = 0.0f;
-        if (n < Cout) {
-            v = dY[(long long)n * M + m];
-            if (relu && Z[m * Np + n] + b[n] <= 0.0f) v = 0.0f;
-        }
-        dZ[i] = __float2bfloat16(v);
-    }
-}
-
-// db[n] = sum_m dZ[m][n]: one block per output channel
-__global__ void k_bias_grad(int M, int Np, const __nv_bfloat16 *__restrict__ dZ, float *__restrict__ db) {
-    __shared__ float red[256];
-    const int n = blockIdx.x;
-    float s = 0.0f;
-    for (long long m = threadIdx.x; m < M; m += blockDim.x) s += __bfloat162float(dZ[m * Np + n]);
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) db[n] = red[0];
-}
-
-// dX[ci][y][x] = sum over taps of dcol[(y - dy) * W + (x - dx)][ci*9 + tap]
-__global__ void k_col2im(int Cin, int H, int W, int Kp, const float *__restrict__ dcol, float *__restrict__ dX) {
-    const long long total = (long long)Cin * H * W;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int ci = (int)(i / ((long long)H * W));
-        const int rem = (int)(i % ((long long)H * W));
-        const int y = rem / W, x = rem % W;
-        float s = 0.0f;
-        for (int r = 0; r < 9; r++) {
-            const int yy = y - (r / 3 - 1), xx = x - (r % 3 - 1);
-            if (yy >= 0 && yy < H && xx >= 0 && xx < W) s += dcol[((long long)yy * W + xx) * Kp + ci * 9 + r];
-        }
-        dX[i] = s;
-    }
+// dY[n][m] = 0 where the layer's ReLU output is 0 (its derivative there)
+__global__ void k_relu_mask(long long count, const float *__restrict__ Y, float *__restrict__ dY) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        if (!(Y[i] > 0.0f)) dY[i] = 0.0f;
 }
 
 // dY = 2 (Y - T) / count; partial sums of the squared error into loss[0]
@@ -406,11 +516,14 @@ __global__ void k_pack_w(int Cin, int Cout, int Kp, int Np, const float *__restr
     }
 }
 
-// g[co][ci*9 + r] = dWt[k][n]
-__global__ void k_unpack_grad(int Cin, int Cout, int Np, const float *__restrict__ dWt, float *__restrict__ g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Cout * Cin * 9; i += gridDim.x * blockDim.x) {
-        const int n = i / (Cin * 9), k = i % (Cin * 9);
-        g[i] = dWt[k * Np + n];
+// Wf[k][n] (bf16) with k = co * 9 + t, n = ci: W[co][ci][8 - t]
+__global__ void k_pack_wflip(int Cin, int Cout, int KpT, int NpT, const float *__restrict__ Wm,
+                             __nv_bfloat16 *__restrict__ Wf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < KpT * NpT; i += gridDim.x * blockDim.x) {
+        const int k = i / NpT, n = i % NpT;
+        const int co = k / 9, t = k % 9;
+        const float v = (k < Cout * 9 && n < Cin) ? Wm[(co * Cin + n) * 9 + (8 - t)] : 0.0f;
+        Wf[i] = __float2bfloat16(v);
     }
 }
 
@@ -438,12 +551,15 @@ struct gr_cnn {
     int64_t n_params = 0;
     float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
     __nv_bfloat16 *wt[kMaxLayers] = {};
-    float *dwt[kMaxLayers] = {};
+    __nv_bfloat16 *wf[kMaxLayers] = {};  // backward operand: Wf[co*9 + t][ci] = W[co][ci][8 - t]
+    int KpT[kMaxLayers] = {}, NpT[kMaxLayers] = {};
+    float *zero_bias = nullptr;
     float *act[kMaxLayers + 1] = {};  // act[0] = input, act[l+1] = output of layer l
-    float *z[kMaxLayers] = {};
-    __nv_bfloat16 *col = nullptr, *dz = nullptr;
-    float *dcol = nullptr, *dact = nullptr, *dact2 = nullptr, *loss = nullptr;
+    float *z[kMaxLayers] = {};  // GEMM output of the fallback path
+    __nv_bfloat16 *col = nullptr;  // patches of a layer too wide for the tensor-core tile (fallback)
+    float *dact = nullptr, *dact2 = nullptr, *loss = nullptr;
     int64_t adam_t = 0;
+    int sm_count = 148;
     int *err = nullptr;  // device: set by a convolution whose accumulator wait gave up
     cudaStream_t stream = nullptr;
 };
@@ -463,6 +579,9 @@ int pack_all(gr_cnn *c) {
     for (int l = 0; l < c->n_layers; l++) {
         k_pack_w<<<grid((long long)c->Kp[l] * c->Np[l]), 256, 0, c->stream>>>(c->cin[l], c->cout[l], c->Kp[l], c->Np[l],
                                                                                c->params + c->w_ofs[l], c->wt[l]);
+        if (l > 0)
+            k_pack_wflip<<<grid((long long)c->KpT[l] * c->NpT[l]), 256, 0, c->stream>>>(
+                c->cin[l], c->cout[l], c->KpT[l], c->NpT[l], c->params + c->w_ofs[l], c->wf[l]);
     }
     CN_CK(cudaGetLastError());
     return GR_OK;
@@ -473,21 +592,16 @@ bool conv_tc_fits(const gr_cnn *c, int l) {
     return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16)) <= kConvSmemMax;
 }
 
-int forward(gr_cnn *c, bool keep_z) {
+int forward(gr_cnn *c) {
     const int M = c->H * c->W;
     cudaStream_t s = c->stream;
-    static bool attr_set = false;  // the attribute holds for the process; one constant value
-    if (!attr_set) {
-        CN_CK(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
-        attr_set = true;
-    }
     for (int l = 0; l < c->n_layers; l++) {
         const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
         if (conv_tc_fits(c, l)) {
             const int Nt = round_up(c->cout[l], 16);
             k_conv_tc<<<(M + kConvRows - 1) / kConvRows, kConvThreads, conv_smem_bytes(c->Kp[l], Nt), s>>>(
                 c->cin[l], c->cout[l], c->H, c->W, c->Kp[l], Nt, c->Np[l], c->act[l], c->wt[l], bl, c->act[l + 1],
-                keep_z ? c->z[l] : nullptr, l + 1 < c->n_layers, c->err);
+                nullptr, l + 1 < c->n_layers, c->err);
             continue;
         }
         k_im2col<<<grid((long long)M * c->Kp[l]), 256, 0, s>>>(c->cin[l], c->H, c->W, c->Kp[l], c->act[l], c->col);
@@ -509,21 +623,19 @@ int backward(gr_cnn *c, const float *d_target) {
     k_mse<<<grid(cnt), 256, 0, s>>>(cnt, c->act[L], d_target, c->dact, c->loss);
     float *dY = c->dact, *dX = c->dact2;
     for (int l = L - 1; l >= 0; l--) {
-        const int relu = l + 1 < L, Kp = c->Kp[l], Np = c->Np[l], cin = c->cin[l], co = c->cout[l];
-        const float *b = c->params + c->w_ofs[l] + (int64_t)co * cin * 9;
-        k_act_grad<<<grid((long long)M * Np), 256, 0, s>>>(M, co, Np, dY, c->z[l], b, c->dz, relu);
-        // the layer's input again as columns (col holds the last layer's)
-        k_im2col<<<grid((long long)M * Kp), 256, 0, s>>>(cin, c->H, c->W, Kp, c->act[l], c->col);
-        CN_CK(cudaMemsetAsync(c->dwt[l], 0, sizeof(float) * Kp * Np, s));
-        int rc = gemm(s, Kp, Np, M, c->col, 1, Kp, c->dz, Np, 1, c->dwt[l], Np, 1, 64);
-        if (rc) return rc;
+        const int cin = c->cin[l], co = c->cout[l], Nt = round_up(co, 16);
+        if (l + 1 < L) k_relu_mask<<<grid((long long)co * M), 256, 0, s>>>((long long)co * M, c->act[l + 1], dY);
         float *g = c->grads + c->w_ofs[l];
-        k_unpack_grad<<<grid((long long)co * cin * 9), 256, 0, s>>>(cin, co, Np, c->dwt[l], g);
-        k_bias_grad<<<co, 256, 0, s>>>(M, Np, c->dz, g + (int64_t)co * cin * 9);
-        if (l > 0) {
-            rc = gemm(s, M, Kp, Np, c->dz, Np, 1, c->wt[l], 1, Np, c->dcol, Kp, 1, 1);
-            if (rc) return rc;
-            k_col2im<<<grid((long long)cin * M), 256, 0, s>>>(cin, c->H, c->W, Kp, c->dcol, dX);
+        CN_CK(cudaMemsetAsync(g, 0, sizeof(float) * (c->w_ofs[l + 1] - c->w_ofs[l]), s));
+        const int ktiles = (9 * cin + 1 + kConvRows - 1) / kConvRows;  // weight rows and the bias row
+        const int want = (2 * c->sm_count + ktiles - 1) / ktiles;
+        const int per = round_up((M + want - 1) / want, kWgPos), splits = (M + per - 1) / per;
+        k_wgrad_tc<<<dim3(splits, ktiles), kConvThreads, wgrad_smem_bytes(Nt), s>>>(cin, co, c->H, c->W, Nt, per,
+                                                                                   c->act[l], dY, g, c->err);
+        if (l > 0) {  // cin = hidden <= 32 and cout <= 32: always within the tensor-core tile
+            k_conv_tc<<<(M + kConvRows - 1) / kConvRows, kConvThreads, conv_smem_bytes(c->KpT[l], round_up(cin, 16)),
+                        s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
+                             dX, nullptr, 0, c->err);
             float *t = dY;
             dY = dX;
             dX = t;
@@ -557,21 +669,24 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
         return GR_ERR_ARG;
     *out = nullptr;
     CN_CK(cudaSetDevice(device));
+    // the attribute holds for the whole process: one constant value
+    CN_CK(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
     gr_cnn *c = new gr_cnn();
     c->device = device;
     c->H = H;
     c->W = W;
     c->n_layers = n_layers;
-    int64_t ofs = 0, kmax = 0, nmax = 0, cmax = in_channels;
+    int64_t ofs = 0, kmax = 0, cmax = in_channels;
     for (int l = 0; l < n_layers; l++) {
         c->cin[l] = l == 0 ? in_channels : hidden;
         c->cout[l] = l + 1 == n_layers ? out_channels : hidden;
         c->Kp[l] = round_up(c->cin[l] * 9, 16);
         c->Np[l] = round_up(c->cout[l], 8);
+        c->KpT[l] = round_up(c->cout[l] * 9, 16);
+        c->NpT[l] = round_up(c->cin[l], 8);
         c->w_ofs[l] = ofs;
         ofs += (int64_t)c->cout[l] * c->cin[l] * 9 + c->cout[l];
-        kmax = c->Kp[l] > kmax ? c->Kp[l] : kmax;
-        nmax = c->Np[l] > nmax ? c->Np[l] : nmax;
+        if (!conv_tc_fits(c, l)) kmax = c->Kp[l] > kmax ? c->Kp[l] : kmax;  // fallback patches
         cmax = c->cout[l] > cmax ? c->cout[l] : cmax;
     }
     c->w_ofs[n_layers] = ofs;
@@ -586,9 +701,10 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
     ok = ok && cudaMalloc(&c->grads, sizeof(float) * ofs) == cudaSuccess;
     ok = ok && cudaMalloc(&c->m1, sizeof(float) * ofs) == cudaSuccess;
     ok = ok && cudaMalloc(&c->m2, sizeof(float) * ofs) == cudaSuccess;
-    ok = ok && cudaMalloc(&c->col, sizeof(__nv_bfloat16) * M * kmax) == cudaSuccess;
-    ok = ok && cudaMalloc(&c->dz, sizeof(__nv_bfloat16) * M * nmax) == cudaSuccess;
-    ok = ok && cudaMalloc(&c->dcol, sizeof(float) * M * kmax) == cudaSuccess;
+    ok = ok && cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
+    if (kmax > 0) ok = ok && cudaMalloc(&c->col, sizeof(__nv_bfloat16) * M * kmax) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->zero_bias, sizeof(float) * 64) == cudaSuccess &&
+         cudaMemset(c->zero_bias, 0, sizeof(float) * 64) == cudaSuccess;
     ok = ok && cudaMalloc(&c->dact, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->dact2, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->loss, sizeof(float) * 2) == cudaSuccess;
@@ -597,8 +713,8 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
         ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
     for (int l = 0; l < n_layers && ok; l++) {
         ok = cudaMalloc(&c->wt[l], sizeof(__nv_bfloat16) * c->Kp[l] * c->Np[l]) == cudaSuccess &&
-             cudaMalloc(&c->z[l], sizeof(float) * M * c->Np[l]) == cudaSuccess &&
-             cudaMalloc(&c->dwt[l], sizeof(float) * c->Kp[l] * c->Np[l]) == cudaSuccess;
+             cudaMalloc(&c->wf[l], sizeof(__nv_bfloat16) * c->KpT[l] * c->NpT[l]) == cudaSuccess;
+        if (ok && !conv_tc_fits(c, l)) ok = cudaMalloc(&c->z[l], sizeof(float) * M * c->Np[l]) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -630,13 +746,13 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
 int gr_cnn_destroy(gr_cnn *c) {
     if (!c) return GR_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (void *p : {(void *)c->params, (void *)c->grads, (void *)c->m1, (void *)c->m2, (void *)c->col, (void *)c->dz,
-                    (void *)c->dcol, (void *)c->dact, (void *)c->dact2, (void *)c->loss, (void *)c->err})
+    for (void *p : {(void *)c->params, (void *)c->grads, (void *)c->m1, (void *)c->m2, (void *)c->col,
+                    (void *)c->zero_bias, (void *)c->dact, (void *)c->dact2, (void *)c->loss, (void *)c->err})
         cudaFree(p);
     for (int l = 0; l < kMaxLayers; l++) {
         cudaFree(c->wt[l]);
+        cudaFree(c->wf[l]);
         cudaFree(c->z[l]);
-        cudaFree(c->dwt[l]);
     }
     for (int l = 0; l <= kMaxLayers; l++) cudaFree(c->act[l]);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -677,7 +793,7 @@ int gr_cnn_forward(gr_cnn *c, const float *d_in, float *d_out) {
     if (!c || !d_in || !d_out) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c, false);
+    int rc = forward(c);
     if (rc) return rc;
     CN_CK(cudaMemcpyAsync(d_out, c->act[c->n_layers], sizeof(float) * M * c->cout[c->n_layers - 1],
                           cudaMemcpyDeviceToDevice, c->stream));
@@ -688,7 +804,7 @@ int gr_cnn_grads(gr_cnn *c, const float *d_in, const float *d_target, float *h_g
     if (!c || !d_in || !d_target) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c, true);
+    int rc = forward(c);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     if (h_grads)
@@ -701,7 +817,7 @@ int gr_cnn_train_step(gr_cnn *c, const float *d_in, const float *d_target, float
     if (!c || !d_in || !d_target || !(lr > 0.0f)) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c, true);
+    int rc = forward(c);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     c->adam_t++;

@@ -123,10 +123,14 @@ def test_forward_matches_reference(cuda, shape):
 
 
 @pytest.mark.gpu
-def test_gradients_match_reference(cuda):
+@pytest.mark.parametrize("shape", [
+    dict(),  # two position ranges of one 64-position stage each
+    dict(H=200, W=200, cin=20, cout=10, hidden=16, layers=3),  # 3 stages per range: both buffers reused
+])
+def test_gradients_match_reference(cuda, shape):
     import torch
 
-    net, x, t = _net_case(seed=5)
+    net, x, t = _net_case(seed=5, **shape)
     p = net.get_params()
     loss, g = net.grads(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
     rloss, rg = cnnref.grads(p, net.layer_shapes(), x, t)
