@@ -29,7 +29,8 @@ GR_PROF_KINDS = 10
 GR_TUNE_MST_MID_THREADS, GR_TUNE_MST_BIG_THREADS, GR_TUNE_MST_CLUSTER_THREADS, GR_TUNE_MST_CLUSTER_MIN_PINS = 0, 1, 2, 3
 GR_TUNE_LPAT_SPLIT = 4
 GR_LA_DEMAND, GR_LA_EXCESS = 0, 1
-GR_TUNE_PARAMS = 5
+GR_TUNE_MST_QUEUE = 5
+GR_TUNE_PARAMS = 6
 
 # every function of include/iitmgr_b200.h: name -> (restype, argtypes)
 _P, _I, _I64, _U64, _D = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double

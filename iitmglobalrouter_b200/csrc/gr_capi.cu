@@ -102,7 +102,9 @@ struct gr_ctx {
     GraphCache graph;
     int64_t launches = 0;
     int mst_smem_max = 0;
-    int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
+    int32_t plan_max_pins = 0;  // largest net of the uploaded plan
+    int *d_queue = nullptr;  // k_mst_queue: next item, CTAs finished (zero between launches)
+    int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
     int levels = 0;  // nodes on the longest Fenwick update path: 1 + floor(log2(max(X, Y)))
     // optional per-kernel timing (CUDA events around every launch)
     bool profiling = false;
@@ -357,6 +359,35 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s,
                bool pin2_done = false) {
     if (v.n <= 0) return GR_OK;
+    if (c->tune[GR_TUNE_MST_QUEUE]) {
+        if (v.n2 > 0 && !pin2_done) {
+            int pi = prof_begin(c, s);
+            k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
+            prof_end(c, s, pi, GR_K_MST);
+        }
+        const int items = v.nl + (v.nm + kQueueWarps - 1) / kQueueWarps;
+        if (items <= 0) return GR_OK;
+        const int maxn = v.nl > 0 ? v.max_pins : kMstWarpPins;
+        const bool in_smem = mst_mat_in_smem(maxn);
+        size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
+        sm = sm > kQueueWarpSmem ? sm : kQueueWarpSmem;
+        int blocks = c->sm_count * (sm <= 100 * 1024 ? 2 : 1);
+        uint32_t *gmat = nullptr;
+        if (!in_smem) {
+            blocks = c->sm_count;
+            if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
+            gmat = (uint32_t *)c->mat.p;
+        }
+        blocks = items < blocks ? items : blocks;
+        BatchView vv = v;
+        vv.max_pins = maxn;
+        int pi = prof_begin(c, s);
+        k_mst_queue<<<blocks, kQueueThreads, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
+                                                      (int64_t)maxn * maxn, c->d_queue);
+        prof_end(c, s, pi, GR_K_MST_LARGE);
+        GR_CK(cudaGetLastError());
+        return GR_OK;
+    }
     // the size classes are independent: warp and larger-net kernels run on
     // side streams forked from s and joined back (parallel graph branches)
     GR_CK(cudaEventRecord(c->ev_fork, s));
@@ -469,7 +500,8 @@ int check_mst_smem(gr_ctx *c, int max_pins) {
 // global pair-cost matrices for k_mst_large when a batch's largest net
 // does not fit in shared memory (one matrix per CTA, at most one CTA per SM)
 int ensure_mst_scratch(gr_ctx *c, int max_pins, cudaStream_t s) {
-    if (max_pins <= kMstMidPins || mst_mat_in_smem(max_pins) || mst_cluster_size(max_pins)) return GR_OK;
+    if (max_pins <= kMstWarpPins || mst_mat_in_smem(max_pins)) return GR_OK;
+    if (!c->tune[GR_TUNE_MST_QUEUE] && (max_pins <= kMstMidPins || mst_cluster_size(max_pins))) return GR_OK;
     return ensure(c->mat, (size_t)c->sm_count * max_pins * max_pins * sizeof(float), s);
 }
 
@@ -613,6 +645,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     // capr is read in aligned 32-cell words: pad it to a whole last word
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4 + 128) || cudaMalloc(&c->d_fen, cell4) ||
         cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_queue, 16) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1)) ||
         cudaMalloc(&c->d_dlut, sizeof(float) * (kLutMax - kLutMin + 2)) ||
         cudaMalloc(&c->d_tbits, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)) ||
@@ -630,7 +663,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
         cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
         cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_list_count, 0, 16) ||
+        cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_queue, 0, 16) ||
         cudaMemset(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)))
         return fail(GR_ERR_CUDA);
     // A function attribute holds for the whole process, not this context:
@@ -654,7 +687,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         cudaFuncSetAttribute(k_mst_cluster<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstClusterSmem))
         return fail(GR_ERR_CUDA);
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
-        cudaSuccess)
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mst_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstSmemMax) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     if ((rc = gr_reset(c, nullptr))) return fail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);
@@ -679,6 +713,7 @@ int gr_destroy(gr_ctx *c) {
     cudaFree(c->d_gdel);
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
+    cudaFree(c->d_queue);
     free_buf(c->mat);
     cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
@@ -719,6 +754,7 @@ int gr_reset(gr_ctx *c, void *stream) {
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
     GR_CK(cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s));
+    GR_CK(cudaMemsetAsync(c->d_queue, 0, 16, s));
     return rebuild_fenwick(c, s);
 }
 
@@ -897,6 +933,7 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     int rc;
     int32_t plan_max_pins = 0;
     for (const BatchInfo &bi : plan) plan_max_pins = bi.max_pins > plan_max_pins ? bi.max_pins : plan_max_pins;
+    c->plan_max_pins = plan_max_pins;
     if ((rc = ensure_mst_scratch(c, plan_max_pins, c->stream))) return rc;
     if ((rc = ensure(c->plan_desc, bytes, c->stream))) return rc;
     GR_CK(cudaMemcpyAsync(c->plan_desc.p, host, bytes, cudaMemcpyHostToDevice, c->stream));
@@ -919,6 +956,12 @@ int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32
     if (!c || !d_mst_edges || b0 < 0 || b1 < b0 || b1 > (int32_t)c->plan.size()) return GR_ERR_ARG;
     if (c->plan.empty() && b1 > 0) return GR_ERR_STATE;
     cudaStream_t s = pick(c, stream);
+    // the Boruvka scratch depends on the launch shapes, which may have changed
+    // since gr_plan_set (a captured graph holds the scratch's address)
+    const void *mat_before = c->mat.p;
+    int rc0 = ensure_mst_scratch(c, c->plan_max_pins, s);
+    if (rc0) return rc0;
+    if (c->mat.p != mat_before) drop_graph(c);
     auto issue = [&]() -> int {
         for (int32_t b = b0; b < b1; b++) {
             const BatchInfo &bi = c->plan[b];
@@ -1136,6 +1179,8 @@ int gr_tune_set(gr_ctx *c, int param, int value) {
         if (value != 0 && (value <= kMstMidPins || value > GR_MAX_PINS)) return GR_ERR_ARG;
     } else if (param == GR_TUNE_LPAT_SPLIT) {
         if (value != 0 && value != 1 && value != 2 && value != 4) return GR_ERR_ARG;
+    } else if (param == GR_TUNE_MST_QUEUE) {
+        if (value != 0 && value != 1) return GR_ERR_ARG;
     } else if (value < 64 || value > 1024 || value % 32) {
         return GR_ERR_ARG;
     }

@@ -503,9 +503,63 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
     return total;
 }
 
-// The net's pair costs are first spread into a full symmetric n x n matrix
-// (shared memory when it fits, else this CTA's global scratch) so that each
-// pin's crossing scan is one coalesced row read by a warp.
+// One net's Boruvka on the whole CTA. The net's pair costs are first spread
+// into a full symmetric n x n matrix M (shared memory when it fits, else this
+// CTA's global scratch) so that each pin's crossing scan is one coalesced row
+// read by a warp.
+__device__ __forceinline__ void mst_block_net(const BatchView &bv, const float *__restrict__ cost,
+                                              int64_t *__restrict__ mst, float *__restrict__ dist, uint32_t *status,
+                                              const MstArrays &a, uint32_t *M, int net, int *warp_sums,
+                                              int *s_total) {
+    const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
+    const int n = bv.npin[net];
+    const long long P = (long long)n * (n - 1) / 2;
+    const float *w = cost + bv.pair_ofs[net];
+    int64_t *out = mst + bv.node_ofs[net];
+    {
+        // four independent loads in flight per thread, then their stores;
+        // (j, k) steps through the pair ids e, e + B, e + 2B, ...
+        int j, k;
+        pair_decode(tid, j, k);
+        for (long long e = tid; e < P; e += 4 * (long long)B) {
+            float c[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) c[i] = e + i * B < P ? __ldg(w + e + i * B) : 0.0f;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                if (e + i * B < P) {
+                    const uint32_t b = cost_bits(c[i]);
+                    M[j * n + k] = b;
+                    M[k * n + j] = b;
+                }
+                k += B;
+                while (k >= j) {
+                    k -= j;
+                    j++;
+                }
+            }
+        }
+    }
+    for (int v = tid; v < n; v += B) a.comp[v] = v;
+    float d = 0.0f;
+    int nrec = 0, rounds = 0;
+    __syncthreads();
+    while (nrec < n - 1 && rounds < kMstMaxRounds) {
+        rounds++;
+        for (int v = tid; v < n; v += B) a.key[v] = ~0ull;
+        __syncthreads();
+        for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * n, v, n, lane);
+        __syncthreads();
+        nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, s_total, status);
+    }
+    for (int v = nrec + tid; v < n; v += B) out[v] = -1;
+    if (tid == 0) {
+        if (dist) dist[net] = d;
+        if (nrec != n - 1) atomicOr(status, 0x4u);
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
                                                    uint32_t *status, uint32_t *__restrict__ gmat, int64_t gmat_stride,
@@ -516,56 +570,8 @@ __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const
     const int maxn = bv.max_pins;
     const MstArrays a = MstArrays::carve(sm, maxn);
     uint32_t *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : (uint32_t *)a.end(maxn);
-    const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
-    for (int t = blockIdx.x; t < count; t += gridDim.x) {
-        const int net = bv.order[first + t];
-        const int n = bv.npin[net];
-        const long long P = (long long)n * (n - 1) / 2;
-        const float *w = cost + bv.pair_ofs[net];
-        int64_t *out = mst + bv.node_ofs[net];
-        {
-            // four independent loads in flight per thread, then their stores;
-            // (j, k) steps through the pair ids e, e + B, e + 2B, ...
-            int j, k;
-            pair_decode(tid, j, k);
-            for (long long e = tid; e < P; e += 4 * (long long)B) {
-                float c[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) c[i] = e + i * B < P ? __ldg(w + e + i * B) : 0.0f;
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    if (e + i * B < P) {
-                        const uint32_t b = cost_bits(c[i]);
-                        M[j * n + k] = b;
-                        M[k * n + j] = b;
-                    }
-                    k += B;
-                    while (k >= j) {
-                        k -= j;
-                        j++;
-                    }
-                }
-            }
-        }
-        for (int v = tid; v < n; v += B) a.comp[v] = v;
-        float d = 0.0f;
-        int nrec = 0, rounds = 0;
-        __syncthreads();
-        while (nrec < n - 1 && rounds < kMstMaxRounds) {
-            rounds++;
-            for (int v = tid; v < n; v += B) a.key[v] = ~0ull;
-            __syncthreads();
-            for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * n, v, n, lane);
-            __syncthreads();
-            nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, &s_total, status);
-        }
-        for (int v = nrec + tid; v < n; v += B) out[v] = -1;
-        if (tid == 0) {
-            if (dist) dist[net] = d;
-            if (nrec != n - 1) atomicOr(status, 0x4u);
-        }
-        __syncthreads();
-    }
+    for (int t = blockIdx.x; t < count; t += gridDim.x)
+        mst_block_net(bv, cost, mst, dist, status, a, M, bv.order[first + t], warp_sums, &s_total);
 }
 
 // Nets whose n x n matrix exceeds one CTA's shared memory: a cluster of CS
@@ -885,50 +891,45 @@ __global__ void k_mst_pin2(BatchView bv, const float *__restrict__ cost, int64_t
 }
 
 // Nets of 3..32 pins: one warp each, pin = lane, the same per-round rule as
-// k_mst_large with the candidate forest resolved by shuffles.
-__global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const float *__restrict__ cost,
-                                                  int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                  uint32_t *status) {
-    __shared__ unsigned long long skey[8][32];
-    __shared__ int scomp[8][32];
-    __shared__ float sw[8][kMstWarpPins * (kMstWarpPins - 1) / 2];
+// k_mst_large with the candidate forest resolved by shuffles. skey/scomp: 32
+// entries, sw: the net's pair costs (kMstWarpPins * (kMstWarpPins - 1) / 2),
+// all in this warp's shared memory.
+__device__ __forceinline__ void mst_warp_net(const BatchView &bv, const float *__restrict__ cost,
+                                             int64_t *__restrict__ mst, float *__restrict__ dist, uint32_t *status,
+                                             int i, unsigned long long *skey, int *scomp, float *sw, int lane) {
     const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int t = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (t >= bv.nm) return;
-    const int i = bv.order[bv.n2 + t];
     const int n = bv.npin[i];
     {
         const float *wg = cost + bv.pair_ofs[i];
-        for (int e = lane; e < n * (n - 1) / 2; e += 32) sw[wib][e] = __ldg(wg + e);
+        for (int e = lane; e < n * (n - 1) / 2; e += 32) sw[e] = __ldg(wg + e);
         __syncwarp();
     }
-    const float *w = sw[wib];
+    const float *w = sw;
     int64_t *out = mst + bv.node_ofs[i];
-    scomp[wib][lane] = lane;
+    scomp[lane] = lane;
     int nrec = 0;
     float d = 0.0f;
     for (int round = 0; nrec < n - 1 && round < kMstMaxRounds; round++) {
-        skey[wib][lane] = ~0ull;
+        skey[lane] = ~0ull;
         __syncwarp();
         if (lane < n) {
-            const int cv = scomp[wib][lane];
+            const int cv = scomp[lane];
             unsigned long long best = ~0ull;
             for (int u = 0; u < n; u++) {
-                if (scomp[wib][u] == cv) continue;
+                if (scomp[u] == cv) continue;
                 const int64_t e = pair_id(lane, u);
                 const unsigned long long kk = cost_key(w[e], (uint32_t)e);
                 best = kk < best ? kk : best;
             }
-            if (best != ~0ull) atomicMin(&skey[wib][cv], best);
+            if (best != ~0ull) atomicMin(&skey[cv], best);
         }
         __syncwarp();
         int sel = -1;
-        const unsigned long long mykey = skey[wib][lane];
-        if (lane < n && scomp[wib][lane] == lane && mykey != ~0ull) {
+        const unsigned long long mykey = skey[lane];
+        if (lane < n && scomp[lane] == lane && mykey != ~0ull) {
             int pj, pk;
             pair_decode((long long)(uint32_t)mykey, pj, pk);
-            sel = scomp[wib][pj] == lane ? scomp[wib][pk] : scomp[wib][pj];
+            sel = scomp[pj] == lane ? scomp[pk] : scomp[pj];
         }
         const int sel_of_sel = __shfl_sync(FULL, sel, sel < 0 ? 0 : sel);
         const bool mutual_top = sel >= 0 && sel_of_sel == lane && lane > sel;
@@ -948,17 +949,83 @@ __global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const f
         for (int it = 0; it < 5; it++) par = __shfl_sync(FULL, par, par);
         const unsigned grp = __match_any_sync(FULL, sel >= 0 ? par : 64 + lane);
         const int newroot = 31 - __clz(grp);
-        const int r_old = scomp[wib][lane];
+        const int r_old = scomp[lane];
         const int sel_r = __shfl_sync(FULL, sel, r_old);
         const int nr_r = __shfl_sync(FULL, newroot, r_old);
         __syncwarp();
-        if (lane < n && sel_r >= 0) scomp[wib][lane] = nr_r;
+        if (lane < n && sel_r >= 0) scomp[lane] = nr_r;
         __syncwarp();
     }
     for (int v = nrec + lane; v < n; v += 32) out[v] = -1;
     if (lane == 0) {
         if (dist) dist[i] = d;
         if (nrec != n - 1) atomicOr(status, 0x4u);
+    }
+}
+
+constexpr int kMstWarpCosts = kMstWarpPins * (kMstWarpPins - 1) / 2;
+
+__global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                  int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                  uint32_t *status) {
+    __shared__ unsigned long long skey[8][32];
+    __shared__ int scomp[8][32];
+    __shared__ float sw[8][kMstWarpCosts];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int t = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (t >= bv.nm) return;
+    mst_warp_net(bv, cost, mst, dist, status, bv.order[bv.n2 + t], skey[wib], scomp[wib], sw[wib], lane);
+}
+
+// ---------------------------------------------------------------- Boruvka, one persistent launch
+// Every net of 3 or more pins of a batch in one launch: CTAs take work items
+// from a queue (an atomic counter) -- first the nets above kMstWarpPins pins,
+// the largest class first, one per item on the whole CTA (mst_block_net),
+// then groups of kQueueWarps nets of 3..32 pins, one per warp
+// (mst_warp_net). The last CTA to find the queue empty resets the counters
+// for the next launch. Shared memory: the block arrays and matrix for the
+// batch's largest net, or the warps' arrays, whichever is larger.
+constexpr int kQueueThreads = 512, kQueueWarps = kQueueThreads / 32;
+constexpr size_t kQueueWarpSmem = (size_t)kQueueWarps * (32 * 8 + 32 * 4 + kMstWarpCosts * 4);
+
+__global__ void __launch_bounds__(kQueueThreads) k_mst_queue(GridC g, BatchView bv, const float *__restrict__ cost,
+                                                            int64_t *__restrict__ mst, float *__restrict__ dist,
+                                                            uint32_t *status, uint32_t *__restrict__ gmat,
+                                                            int64_t gmat_stride, int *__restrict__ queue) {
+    extern __shared__ unsigned long long sm[];
+    __shared__ int warp_sums[32];
+    __shared__ int s_total, s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int maxn = bv.max_pins;
+    const MstArrays a = MstArrays::carve(sm, maxn);
+    uint32_t *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : (uint32_t *)a.end(maxn);
+    unsigned long long *skey = sm + warp * 32;
+    int *scomp = (int *)(sm + kQueueWarps * 32) + warp * 32;
+    float *sw = (float *)((int *)(sm + kQueueWarps * 32) + kQueueWarps * 32) + warp * kMstWarpCosts;
+    const int nbig = bv.nl - bv.nmid, nlarge = bv.nl;
+    const int total = nlarge + (bv.nm + kQueueWarps - 1) / kQueueWarps;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        if (item < nlarge) {  // nets above 128 pins first, then 33..128
+            const int t = item < nbig ? bv.nmid + item : item - nbig;
+            mst_block_net(bv, cost, mst, dist, status, a, M, bv.order[bv.n2 + bv.nm + t], warp_sums, &s_total);
+        } else {
+            const int t = (item - nlarge) * kQueueWarps + warp;
+            if (t < bv.nm) mst_warp_net(bv, cost, mst, dist, status, bv.order[bv.n2 + t], skey, scomp, sw, lane);
+            __syncthreads();
+        }
+    }
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+            __threadfence();
+        }
     }
 }
 

@@ -19,7 +19,7 @@ import json
 from pathlib import Path
 
 from ._capi import (GR_TUNE_LPAT_SPLIT, GR_TUNE_MST_BIG_THREADS, GR_TUNE_MST_CLUSTER_MIN_PINS,
-                    GR_TUNE_MST_CLUSTER_THREADS, GR_TUNE_MST_MID_THREADS)
+                    GR_TUNE_MST_CLUSTER_THREADS, GR_TUNE_MST_MID_THREADS, GR_TUNE_MST_QUEUE)
 
 NAMES = {
     GR_TUNE_MST_MID_THREADS: "mst_mid_threads",
@@ -27,6 +27,7 @@ NAMES = {
     GR_TUNE_MST_CLUSTER_THREADS: "mst_cluster_threads",
     GR_TUNE_MST_CLUSTER_MIN_PINS: "mst_cluster_min_pins",
     GR_TUNE_LPAT_SPLIT: "lpat_split",
+    GR_TUNE_MST_QUEUE: "mst_queue",
 }
 CANDIDATES = {
     GR_TUNE_MST_MID_THREADS: [128, 256, 512, 1024],
@@ -34,6 +35,7 @@ CANDIDATES = {
     GR_TUNE_MST_CLUSTER_THREADS: [256, 512, 1024],
     GR_TUNE_MST_CLUSTER_MIN_PINS: [0, 129, 160, 192],
     GR_TUNE_LPAT_SPLIT: [0, 1, 2, 4],
+    GR_TUNE_MST_QUEUE: [0, 1],
 }
 DEFAULT_PATH = Path(__file__).resolve().parent / "tuning.json"
 

@@ -211,7 +211,11 @@ int gr_route_design_lookahead_host(gr_ctx *ctx, gr_cnn *cnn, int32_t every, floa
                                           when one CTA could hold them (0: never) */
 #define GR_TUNE_LPAT_SPLIT 4           /* warps sharing a group of 32 pairs in the
                                           L-pattern kernel: 1, 2, 4 (0: by batch size) */
-#define GR_TUNE_PARAMS 5
+#define GR_TUNE_MST_QUEUE 5            /* 1: every net of 3+ pins of a batch in one
+                                          persistent launch fed by a work queue
+                                          (k_mst_queue); 0: one kernel per
+                                          pin-count class on parallel streams */
+#define GR_TUNE_PARAMS 6
 int gr_tune_set(gr_ctx *ctx, int param, int value); /* threads: 64..1024, multiple of 32 */
 /* (results do not depend on any of them; the L-pattern split only on latency) */
 int gr_tune_get(gr_ctx *ctx, int param, int *value);

@@ -124,15 +124,17 @@ def test_brvsk_boundary_bitexact(cuda):
         assert np.array_equal(bits(dist.cpu().numpy()), bits(dist_c))
 
 
-# (mid threads, big threads, cluster threads, cluster from pins)
-TUNINGS = [(128, 256, 256, 0), (1024, 1024, 1024, 129), (256, 512, 512, 200), (64, 64, 64, 0)]
+# (mid threads, big threads, cluster threads, cluster from pins[, L-pattern split, persistent queue])
+TUNINGS = [(128, 256, 256, 0), (1024, 1024, 1024, 129), (256, 512, 512, 200), (64, 64, 64, 0),
+           (1024, 1024, 1024, 129, 0, 1)]
 
 
 @pytest.mark.parametrize("tuning", TUNINGS)
 def test_brvsk_launch_shapes_do_not_change_results(cuda, tuning):
     """Every Boruvka launch shape gives the oracle's trees bit for bit: nets
     in the mid class, single-CTA big nets, 4- and 8-CTA clusters and the
-    global-matrix path (700 pins)."""
+    global-matrix path (700 pins); and the persistent queue kernel, which
+    takes all of them (the 700-pin net through its global matrix)."""
     import torch
 
     X, Y, Z = 48, 48, 4
@@ -161,7 +163,7 @@ def test_brvsk_launch_shapes_do_not_change_results(cuda, tuning):
 
 def test_tune_rejects_bad_values(cuda):
     R = gr.Router(8, 8, 3, np.ones(192, np.int32))
-    for p, v in [(0, 48), (0, 2048), (1, 100), (3, 100), (3, 5000), (4, 3), (4, 8), (7, 512)]:
+    for p, v in [(0, 48), (0, 2048), (1, 100), (3, 100), (3, 5000), (4, 3), (4, 8), (5, 2), (5, -1), (7, 512)]:
         with pytest.raises(gr.GRError):
             R.tune_set(p, v)
 
@@ -225,6 +227,35 @@ def test_route_config1_bitexact(cuda, mode):
     assert np.array_equal(R.demand(), g.demand())
     assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))
     assert R.status() == 0
+
+
+@pytest.mark.parametrize("mode", ["plan", "graph"])
+def test_route_persistent_queue_bitexact(cuda, mode):
+    """The whole 64x64x5 route and the first batches of the 400x400x9 design
+    with every batch's Boruvka stage in one persistent queue launch: the
+    oracle's trees, patterns, capacities and Fenwick nodes."""
+    from iitmglobalrouter_b200._capi import GR_TUNE_MST_QUEUE
+
+    for config, n_nets, nb in ((1, 0, None), (2, 40000, 3)):
+        d = gr.Design.generate(config, seed=2, n_nets=n_nets)
+        X, Y, Z, cap, ofs, pins = design_arrays(d)
+        bofs, ids = d.batch(4)
+        if nb is not None:
+            bofs, ids = bofs[: nb + 1], ids[: bofs[nb]]
+        g = oracle.Grid(X, Y, Z, cap)
+        rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=NT)
+        assert rc == 0
+        R = gr.Router(X, Y, Z, cap)
+        R.set_nets(ofs, pins)
+        R.tune_set(GR_TUNE_MST_QUEUE, 1)
+        for _ in range(2):  # the queue counters are back at zero for the second route
+            R.reset()
+            mst, mp = route_all_gpu(R, ofs, bofs, ids, mode)
+            assert np.array_equal(mst, mst_c)
+            assert np.array_equal(mp, mp_c)
+            assert np.array_equal(R.capr(), g.capr())
+            assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))
+            assert R.status() == 0
 
 
 def test_route_config2_first_batches_bitexact(cuda):

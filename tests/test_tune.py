@@ -68,5 +68,7 @@ def test_candidates_are_valid_values(p):
             assert v == 0 or 128 < v <= 4096
         elif p == 4:
             assert v in (0, 1, 2, 4)
+        elif p == 5:
+            assert v in (0, 1)
         else:
             assert 64 <= v <= 1024 and v % 32 == 0
