@@ -214,35 +214,50 @@ __global__ void __launch_bounds__(kConvThreads, 2)
         *(uint4 *)(Bs + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 
-    // patches: thread (row r, half h) fills k chunks [h * nchunk / 2, (h + 1) * nchunk / 2) of row r
+    // patches: thread (row r, half h) fills the channel groups g = h, h + 2, ...
+    // of row r. A group of 8 channels is 72 k values = 9 whole chunks, so the
+    // fully unrolled loop has every element's channel, tap and word position
+    // fixed at compile time; a tap outside the grid, a row past M and a
+    // channel past cin read as zero, and chunks past Kp are not stored.
     {
         const int r = tid & (kConvRows - 1), h = tid >> 7;
         const int m = m0 + r;
-        const int c0 = h * (nchunk >> 1), c1 = h ? nchunk : (nchunk >> 1);  // nchunk is even (Kp % 16 == 0)
         const int y = m < M ? m / W : 0, x = m < M ? m - y * W : 0;
-        int vmask = 0;  // bit dy * 3 + dx: tap inside the grid
+        int vmask = 0;  // bit t = dy * 3 + dx: tap inside the grid
+        int off[9];
 #pragma unroll
         for (int t = 0; t < 9; t++) {
             const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
             vmask |= (m < M && yy >= 0 && yy < H && xx >= 0 && xx < W) << t;
+            off[t] = (t / 3 - 1) * W + (t % 3 - 1);
         }
-        int ci = (8 * c0) / 9, tap = 8 * c0 - 9 * ci;
-        for (int c = c0; c < c1; c++) {
+        const int ngroups = (cin + 7) >> 3;
+        uint8_t *arow = As + r * 16;
+        for (int gi = h; gi < ngroups; gi += 2) {
+            const float *base = X + (long long)(gi * 8) * M + m;
+            const int nch = cin - gi * 8;  // channels of this group that exist (may exceed 8)
             uint32_t w[4];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                float v = 0.0f;
-                if (ci < cin && ((vmask >> tap) & 1)) {
-                    const int dy = tap / 3, dx = tap - 3 * dy;
-                    v = __ldg(X + (long long)ci * M + m + (dy - 1) * W + (dx - 1));
+            for (int e = 0; e < 72; e += 2) {
+                float v[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int j = (e + u) / 9, t = (e + u) % 9;
+                    const bool ok = j < nch && ((vmask >> t) & 1);
+                    v[u] = ok ? __ldg(base + (long long)j * M + off[t]) : 0.0f;
                 }
-                const uint32_t b = __bfloat16_as_ushort(__float2bfloat16(v));
-                if (j & 1) w[j >> 1] |= b << 16;
-                else w[j >> 1] = b;
-                if (++tap == 9) tap = 0, ci++;
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[0], v[1]);
+                w[(e >> 1) & 3] = *reinterpret_cast<const uint32_t *>(&b2);
+                if (((e >> 1) & 3) == 3) {
+                    const int c = gi * 9 + (e >> 3);
+                    if (c < nchunk)
+                        *(uint4 *)(arow + (size_t)c * (kConvRows * 16)) = make_uint4(w[0], w[1], w[2], w[3]);
+                }
             }
-            *(uint4 *)(As + (size_t)c * (kConvRows * 16) + r * 16) = make_uint4(w[0], w[1], w[2], w[3]);
         }
+        // zero chunks past the last group (Kp = 80 for cin = 8, say)
+        for (int c = (ngroups * 9) + h; c < nchunk; c += 2)
+            *(uint4 *)(arow + (size_t)c * (kConvRows * 16)) = make_uint4(0u, 0u, 0u, 0u);
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -364,14 +379,29 @@ __global__ void __launch_bounds__(kConvThreads, 2)
                 const int ci = r / 9, t = r - 9 * ci, dy = t / 3 - 1, dx = t - 3 * (t / 3) - 1;
                 int y = p / W, x = p - y * W;
                 const float *Xc = X + (long long)ci * M;
+                float v[8];
+                const int yy = y + dy;
+                if (p + 8 <= p1 && x + 8 <= W) {  // one image row: one row check, edge checks at both ends
+                    const bool row_ok = yy >= 0 && yy < H;
+                    const float *src = Xc + (long long)yy * W + x + dx;
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int yy = y + dy, xx = x + dx;
-                    float v = 0.0f;
-                    if (p + j < p1 && yy >= 0 && yy < H && xx >= 0 && xx < W) v = __ldg(Xc + yy * W + xx);
-                    const uint32_t h = __bfloat16_as_ushort(__float2bfloat16(v));
-                    w[j >> 1] |= (j & 1) ? h << 16 : h;
-                    if (++x == W) x = 0, y++;
+                    for (int j = 0; j < 8; j++) {
+                        const int xx = x + j + dx;
+                        v[j] = (row_ok && xx >= 0 && xx < W) ? __ldg(src + j) : 0.0f;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const int yj = y + dy, xx = x + dx;
+                        v[j] = (p + j < p1 && yj >= 0 && yj < H && xx >= 0 && xx < W) ? __ldg(Xc + yj * W + xx)
+                                                                                       : 0.0f;
+                        if (++x == W) x = 0, y++;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    w[j] = *reinterpret_cast<const uint32_t *>(&b2);
                 }
             } else if (r == K9) {
                 const uint32_t one = __bfloat16_as_ushort(__float2bfloat16(1.0f));
@@ -386,12 +416,19 @@ __global__ void __launch_bounds__(kConvThreads, 2)
             const int n = i % Nt, ch = i / Nt, p = pb + ch * 8;
             uint32_t w[4] = {0u, 0u, 0u, 0u};
             if (n < cout) {
-                const float *dz = dZ + (long long)n * M;
+                const float *dz = dZ + (long long)n * M + p;
+                float v[8];
+                if (p + 8 <= p1 && ((uintptr_t)dz & 15) == 0) {
+                    const float4 a = __ldg((const float4 *)dz), b4 = __ldg((const float4 *)dz + 1);
+                    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b4.x, v[5] = b4.y, v[6] = b4.z, v[7] = b4.w;
+                } else {
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const float v = p + j < p1 ? __ldg(dz + p + j) : 0.0f;
-                    const uint32_t h = __bfloat16_as_ushort(__float2bfloat16(v));
-                    w[j >> 1] |= (j & 1) ? h << 16 : h;
+                    for (int j = 0; j < 8; j++) v[j] = p + j < p1 ? __ldg(dz + j) : 0.0f;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    w[j] = *reinterpret_cast<const uint32_t *>(&b2);
                 }
             }
             *(uint4 *)(Bs0 + b * b_bytes + ch * (Nt * 16) + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
