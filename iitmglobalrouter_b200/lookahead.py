@@ -64,14 +64,25 @@ class LookaheadNet:
         check(self._lib.gr_cnn_set_params(self._h, ptr(p)), "gr_cnn_set_params")
 
     def _check_in(self, x):
-        assert x.is_cuda and x.dtype.is_floating_point and x.is_contiguous()
+        import torch
+
+        assert x.is_cuda and x.dtype == torch.float32 and x.is_contiguous()
         assert tuple(x.shape) == (self.in_channels, self.H, self.W), x.shape
+
+    @staticmethod
+    def _torch_done(x):
+        """The network runs on its own stream: whatever torch's stream still
+        has queued on x (or on memory it hands out next) finishes first."""
+        import torch
+
+        torch.cuda.current_stream(x.device).synchronize()
 
     def forward(self, x):
         import torch
 
         self._check_in(x)
         y = torch.empty((self.out_channels, self.H, self.W), dtype=torch.float32, device=x.device)
+        self._torch_done(x)
         check(self._lib.gr_cnn_forward(self._h, x.data_ptr(), y.data_ptr()), "gr_cnn_forward")
         return y
 
@@ -80,12 +91,14 @@ class LookaheadNet:
         self._check_in(x)
         g = np.empty(self.num_params, dtype=np.float32)
         loss = np.zeros(1, dtype=np.float32)
+        self._torch_done(x)
         check(self._lib.gr_cnn_grads(self._h, x.data_ptr(), target.data_ptr(), ptr(g), ptr(loss)), "gr_cnn_grads")
         return float(loss[0]), g
 
     def train_step(self, x, target, lr: float = 1e-3) -> float:
         self._check_in(x)
         loss = np.zeros(1, dtype=np.float32)
+        self._torch_done(x)
         check(self._lib.gr_cnn_train_step(self._h, x.data_ptr(), target.data_ptr(), C.c_float(lr), ptr(loss)),
               "gr_cnn_train_step")
         return float(loss[0])
