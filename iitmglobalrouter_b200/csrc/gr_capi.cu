@@ -660,11 +660,15 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     std::vector<float> lut(kLutMax - kLutMin + 1);
     for (int cc = kLutMin; cc <= kLutMax; cc++) lut[cc - kLutMin] = (float)std::exp(-0.5 * (double)cc);
     c->h_cap0.assign(h_cap, h_cap + csize);
-    if (cudaMemcpy(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice) ||
-        cudaMemcpy(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice) ||
-        cudaMemset(c->d_mark, 0, words * 4) || cudaMemset(c->d_status, 0, 16) ||
-        cudaMemset(c->d_list_count, 0, 16) || cudaMemset(c->d_queue, 0, 16) ||
-        cudaMemset(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)))
+    // every upload and clear on the context's own (non-blocking) stream: a
+    // legacy-stream cudaMemcpy from pageable memory may return before its DMA
+    // lands, and nothing orders the legacy stream before this one
+    const cudaStream_t s0 = c->stream;
+    if (cudaMemcpyAsync(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice, s0) ||
+        cudaMemcpyAsync(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice, s0) ||
+        cudaMemsetAsync(c->d_mark, 0, words * 4, s0) || cudaMemsetAsync(c->d_status, 0, 16, s0) ||
+        cudaMemsetAsync(c->d_list_count, 0, 16, s0) || cudaMemsetAsync(c->d_queue, 0, 16, s0) ||
+        cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s0))
         return fail(GR_ERR_CUDA);
     // A function attribute holds for the whole process, not this context:
     // set it to the most any context launches with, so that a context for a
@@ -1082,7 +1086,8 @@ int gr_clear_status(gr_ctx *c) {
 int gr_get_capr(gr_ctx *c, int32_t *h_out) {
     if (!c || !h_out) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
-    GR_CK(cudaMemcpy(h_out, c->d_capr, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToHost));
+    GR_CK(cudaMemcpyAsync(h_out, c->d_capr, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToHost, c->stream));
+    GR_CK(cudaStreamSynchronize(c->stream));
     return GR_OK;
 }
 
@@ -1096,7 +1101,8 @@ int gr_get_demand(gr_ctx *c, int32_t *h_out) {
 int gr_get_fenwick(gr_ctx *c, float *h_out) {
     if (!c || !h_out) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
-    GR_CK(cudaMemcpy(h_out, c->d_fen, sizeof(float) * c->csize, cudaMemcpyDeviceToHost));
+    GR_CK(cudaMemcpyAsync(h_out, c->d_fen, sizeof(float) * c->csize, cudaMemcpyDeviceToHost, c->stream));
+    GR_CK(cudaStreamSynchronize(c->stream));
     return GR_OK;
 }
 

@@ -689,7 +689,8 @@ int finish(gr_cnn *c) {
     CN_CK(cudaMemcpyAsync(&err, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CN_CK(cudaStreamSynchronize(c->stream));
     if (err) {
-        CN_CK(cudaMemset(c->err, 0, sizeof(int)));
+        CN_CK(cudaMemsetAsync(c->err, 0, sizeof(int), c->stream));
+        CN_CK(cudaStreamSynchronize(c->stream));
         return GR_ERR_DEVICE;
     }
     return GR_OK;
@@ -740,12 +741,16 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
     ok = ok && cudaMalloc(&c->m2, sizeof(float) * ofs) == cudaSuccess;
     ok = ok && cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) == cudaSuccess;
     if (kmax > 0) ok = ok && cudaMalloc(&c->col, sizeof(__nv_bfloat16) * M * kmax) == cudaSuccess;
+    // uploads and clears on the network's own (non-blocking) stream: a
+    // legacy-stream cudaMemcpy from pageable memory may return before its
+    // DMA lands, and nothing orders the legacy stream before this one
     ok = ok && cudaMalloc(&c->zero_bias, sizeof(float) * 64) == cudaSuccess &&
-         cudaMemset(c->zero_bias, 0, sizeof(float) * 64) == cudaSuccess;
+         cudaMemsetAsync(c->zero_bias, 0, sizeof(float) * 64, c->stream) == cudaSuccess;
     ok = ok && cudaMalloc(&c->dact, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->dact2, sizeof(float) * M * cmax) == cudaSuccess;
     ok = ok && cudaMalloc(&c->loss, sizeof(float) * 2) == cudaSuccess;
-    ok = ok && cudaMalloc(&c->err, sizeof(int)) == cudaSuccess && cudaMemset(c->err, 0, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc(&c->err, sizeof(int)) == cudaSuccess &&
+         cudaMemsetAsync(c->err, 0, sizeof(int), c->stream) == cudaSuccess;
     for (int l = 0; l <= n_layers && ok; l++)
         ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
     for (int l = 0; l < n_layers && ok; l++) {
@@ -771,9 +776,9 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
         const double a = std::sqrt(6.0 / (c->cin[l] * 9.0));
         for (int64_t i = 0; i < (int64_t)c->cout[l] * c->cin[l] * 9; i++) h[c->w_ofs[l] + i] = (float)((2 * rnd() - 1) * a);
     }
-    if (cudaMemcpy(c->params, h.data(), sizeof(float) * ofs, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(c->m1, 0, sizeof(float) * ofs) != cudaSuccess ||
-        cudaMemset(c->m2, 0, sizeof(float) * ofs) != cudaSuccess || pack_all(c) != GR_OK ||
+    if (cudaMemcpyAsync(c->params, h.data(), sizeof(float) * ofs, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->m1, 0, sizeof(float) * ofs, c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->m2, 0, sizeof(float) * ofs, c->stream) != cudaSuccess || pack_all(c) != GR_OK ||
         cudaStreamSynchronize(c->stream) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     *out = c;
@@ -812,14 +817,15 @@ int gr_cnn_info(gr_cnn *c, int *device, int *in_channels, int *out_channels, int
 int gr_cnn_get_params(gr_cnn *c, float *h_out) {
     if (!c || !h_out) return GR_ERR_ARG;
     CN_CK(cudaStreamSynchronize(c->stream));
-    CN_CK(cudaMemcpy(h_out, c->params, sizeof(float) * c->n_params, cudaMemcpyDeviceToHost));
+    CN_CK(cudaMemcpyAsync(h_out, c->params, sizeof(float) * c->n_params, cudaMemcpyDeviceToHost, c->stream));
+    CN_CK(cudaStreamSynchronize(c->stream));
     return GR_OK;
 }
 
 int gr_cnn_set_params(gr_cnn *c, const float *h_in) {
     if (!c || !h_in) return GR_ERR_ARG;
     CN_CK(cudaStreamSynchronize(c->stream));
-    CN_CK(cudaMemcpy(c->params, h_in, sizeof(float) * c->n_params, cudaMemcpyHostToDevice));
+    CN_CK(cudaMemcpyAsync(c->params, h_in, sizeof(float) * c->n_params, cudaMemcpyHostToDevice, c->stream));
     int rc = pack_all(c);
     if (rc) return rc;
     CN_CK(cudaStreamSynchronize(c->stream));

@@ -167,23 +167,41 @@ class Router:
         self._pin_ofs = pin_ofs
 
     # ---------------------------------------------------------- boundaries
+    @staticmethod
+    def _after_torch(stream, *tensors):
+        """With stream None the library works on the context's own stream:
+        torch work still queued on the tensors handed over (a fill, a copy)
+        finishes first."""
+        if stream is not None:
+            return
+        for t in tensors:
+            if t is not None and getattr(t, "is_cuda", False):
+                import torch
+
+                torch.cuda.current_stream(t.device).synchronize()
+                return
+
     def lpattern(self, pairs, cost, pat, stream=None):
         """pairs: CUDA int32 [2P]; cost: CUDA float32 [P]; pat: CUDA int16 [P]."""
         n = pairs.numel() // 2
+        self._after_torch(stream, pairs, cost, pat)
         check(self._lib.gr_lpattern(self._h, ptr(pairs), n, ptr(cost), ptr(pat), stream), "gr_lpattern")
 
     def brvsk_build(self, net_ids, pair_cost, mst, dist=None, stream=None):
         ids = i32(net_ids)
+        self._after_torch(stream, pair_cost, mst, dist)
         check(self._lib.gr_brvsk_build(self._h, ptr(ids), len(ids), ptr(pair_cost), ptr(mst), ptr(dist), stream),
               "gr_brvsk_build")
 
     def mst_bit_commit(self, net_ids, mst, pair_pat, mst_pat=None, stream=None):
         ids = i32(net_ids)
+        self._after_torch(stream, mst, pair_pat, mst_pat)
         check(self._lib.gr_mst_bit_commit(self._h, ptr(ids), len(ids), ptr(mst), ptr(pair_pat), ptr(mst_pat),
                                           stream), "gr_mst_bit_commit")
 
     def route_batch(self, net_ids, mst, mst_pat=None, dist=None, pair_cost=None, pair_pat=None, stream=None):
         ids = i32(net_ids)
+        self._after_torch(stream, mst, mst_pat, dist, pair_cost, pair_pat)
         check(self._lib.gr_route_batch(self._h, ptr(ids), len(ids), ptr(mst), ptr(mst_pat), ptr(dist),
                                        ptr(pair_cost), ptr(pair_pat), stream), "gr_route_batch")
 
@@ -199,6 +217,7 @@ class Router:
 
     def route_plan(self, mst, mst_pat=None, b0=0, b1=None, graph=False, stream=None):
         b1 = self.n_batches if b1 is None else b1
+        self._after_torch(stream, mst, mst_pat)
         check(self._lib.gr_route_plan(self._h, b0, b1, ptr(mst), ptr(mst_pat), GR_PLAN_GRAPH if graph else 0,
                                       stream), "gr_route_plan")
 
