@@ -322,7 +322,8 @@ __global__ void __launch_bounds__(kConvThreads, 2)
 //   B[n][p] = dZ[n][p] (channel-major fp32, already masked by the ReLU derivative)
 // Stages of 64 positions (four K = 16 MMAs) are gathered into one of two
 // shared-memory buffers while the tensor core consumes the other; each
-// buffer's MMAs are committed to its own mbarrier. The 128 x Nt partial sums
+// buffer's MMAs are committed to its own mbarrier. CTAs split the positions
+// (about four per SM, to hide the gathers' latency). The 128 x Nt partial sums
 // are added (atomics) into the gradient in parameter layout: g[n][r] for the
 // weights, g[cout * 9 cin + n] for the bias.
 constexpr int kWgPos = 64;
@@ -665,7 +666,7 @@ int backward(gr_cnn *c, const float *d_target) {
         float *g = c->grads + c->w_ofs[l];
         CN_CK(cudaMemsetAsync(g, 0, sizeof(float) * (c->w_ofs[l + 1] - c->w_ofs[l]), s));
         const int ktiles = (9 * cin + 1 + kConvRows - 1) / kConvRows;  // weight rows and the bias row
-        const int want = (2 * c->sm_count + ktiles - 1) / ktiles;
+        const int want = (4 * c->sm_count + ktiles - 1) / ktiles;  // 4 CTAs per SM fit (42 KB, 56 registers)
         const int per = round_up((M + want - 1) / want, kWgPos), splits = (M + per - 1) / per;
         k_wgrad_tc<<<dim3(splits, ktiles), kConvThreads, wgrad_smem_bytes(Nt), s>>>(cin, co, c->H, c->W, Nt, per,
                                                                                    c->act[l], dY, g, c->err);
