@@ -13,6 +13,8 @@
 #include <mutex>
 #include <vector>
 
+#include <omp.h>
+
 #include "../../include/iitmgr_b200.h"
 #include "gr_kernels.cuh"
 
@@ -80,6 +82,7 @@ struct gr_ctx {
     void *h_stage = nullptr;
     size_t h_stage_bytes = 0;
     cudaEvent_t stage_done = nullptr;
+    cudaEvent_t nets_up = nullptr;  // gr_set_nets: the caller's buffers uploaded
     cudaStream_t side[3] = {};       // concurrent Boruvka size classes (graph branches when captured)
     cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
     float *d_dlut = nullptr;  // cost(c-1) - cost(c), c = kLutMin .. kLutMax+1
@@ -103,6 +106,8 @@ struct gr_ctx {
     int64_t launches = 0;
     int mst_smem_max = 0;
     int32_t plan_max_pins = 0;  // largest net of the uploaded plan
+    DevBuf plan_ids, plan_bofs, plan_pb;  // device plan builder: inputs, per-batch totals and an error flag
+    bool h_nxy_valid = false;             // h_nxy mirrors d_nxy (copied when a host-built descriptor needs it)
     int *d_queue = nullptr;  // k_mst_queue: next item, CTAs finished (zero between launches)
     int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
     int levels = 0;  // nodes on the longest Fenwick update path: 1 + floor(log2(max(X, Y)))
@@ -516,9 +521,24 @@ int ensure_scratch(gr_ctx *c, int64_t pairs, int64_t tab, int64_t nets, cudaStre
 }
 
 // copies the descriptor of a per-call batch to the device; returns its info
+// the host mirror of the per-net table shapes (for descriptors built on the host)
+int ensure_h_nxy(gr_ctx *c) {
+    if (c->h_nxy_valid) return GR_OK;
+    c->h_nxy.resize(c->n_nets);
+    if (c->n_nets > 0) {
+        GR_CK(cudaMemcpyAsync(c->h_nxy.data(), c->d_nxy, sizeof(int32_t) * c->n_nets, cudaMemcpyDeviceToHost,
+                              c->stream));
+        GR_CK(cudaStreamSynchronize(c->stream));
+    }
+    c->h_nxy_valid = true;
+    return GR_OK;
+}
+
 int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchView &v, cudaStream_t s) {
     if (!c->d_pins) return GR_ERR_STATE;
     if (n < 0 || (n > 0 && !ids)) return GR_ERR_ARG;
+    int rc0 = ensure_h_nxy(c);
+    if (rc0) return rc0;
     size_t bytes = desc_bytes(n > 0 ? n : 1);
     if (bytes > c->h_stage_bytes) {
         if (c->h_stage) {
@@ -629,7 +649,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(GR_ERR_CUDA);
-    if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
+    if (cudaEventCreateWithFlags(&c->stage_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->nets_up, cudaEventDisableTiming) != cudaSuccess)
+        return fail(GR_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess)
@@ -733,6 +755,7 @@ int gr_destroy(gr_ctx *c) {
     if (c->h_stage) cudaFreeHost(c->h_stage);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
     if (c->stage_done) cudaEventDestroy(c->stage_done);
+    if (c->nets_up) cudaEventDestroy(c->nets_up);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
     if (c->ev_out) cudaEventDestroy(c->ev_out);
@@ -740,6 +763,9 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->out_pat);
     free_buf(c->la_feat);
     free_buf(c->la_out);
+    free_buf(c->plan_ids);
+    free_buf(c->plan_bofs);
+    free_buf(c->plan_pb);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -810,21 +836,37 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
         }
         c->nets_cap = (size_t)(n_nets + 1);
     }
+    GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    // nets above 32 pins (k_coords_block), in net order, gathered per thread while the pins upload
     std::vector<int32_t> big;
     int32_t big_max = 0;
-    for (int32_t i = 0; i < n_nets; i++) {
-        const int32_t k = (int32_t)(h_pin_ofs[i + 1] - h_pin_ofs[i]);
-        if (k > 32) {
-            big.push_back(i);
-            big_max = k > big_max ? k : big_max;
+#pragma omp parallel
+    {
+        std::vector<int32_t> mine;
+        int32_t mx = 0;
+#pragma omp for schedule(static) nowait
+        for (int32_t i = 0; i < n_nets; i++) {
+            const int32_t k = (int32_t)(h_pin_ofs[i + 1] - h_pin_ofs[i]);
+            if (k > 32) {
+                mine.push_back(i);
+                mx = k > mx ? k : mx;
+            }
+        }
+#pragma omp for ordered schedule(static, 1)
+        for (int t = 0; t < omp_get_num_threads(); t++) {
+#pragma omp ordered
+            {
+                big.insert(big.end(), mine.begin(), mine.end());
+                big_max = mx > big_max ? mx : big_max;
+            }
         }
     }
-    GR_CK(cudaMemcpyAsync(c->d_pins, h_pins, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
     GR_CK(cudaMemcpyAsync(c->d_pin_ofs, h_pin_ofs, sizeof(int64_t) * (n_nets + 1), cudaMemcpyHostToDevice,
                           c->stream));
     if (!big.empty())
         GR_CK(cudaMemcpyAsync(c->d_big, big.data(), sizeof(int32_t) * big.size(), cudaMemcpyHostToDevice,
                               c->stream));
+    GR_CK(cudaEventRecord(c->nets_up, c->stream));
     if (n_nets > 0) {
         k_coords_warp<<<(int)(((int64_t)n_nets * 32 + 255) / 256), 256, 0, c->stream>>>(
             c->g, n_nets, c->d_pin_ofs, c->d_pins, c->d_pxy, c->d_cx, c->d_cy, c->d_nxy);
@@ -836,14 +878,13 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
         c->launches++;
     }
     GR_CK(cudaGetLastError());
-    c->h_nxy.resize(n_nets);
-    if (n_nets > 0)
-        GR_CK(cudaMemcpyAsync(c->h_nxy.data(), c->d_nxy, sizeof(int32_t) * n_nets, cudaMemcpyDeviceToHost,
-                              c->stream));
+    c->h_nxy_valid = false;  // copied back when a host-built descriptor needs it
     c->h_pin_ofs.assign(h_pin_ofs, h_pin_ofs + n_nets + 1);
     c->n_nets = n_nets;
     c->plan.clear();
-    GR_CK(cudaStreamSynchronize(c->stream));
+    // the caller's buffers are free once their uploads are done; the
+    // coordinate kernels run on (later work on the stream is ordered after them)
+    GR_CK(cudaEventSynchronize(c->nets_up));
     return GR_OK;
 }
 
@@ -904,29 +945,61 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
         if (h_batch_ofs[b + 1] < h_batch_ofs[b]) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
     drop_graph(c);
-    size_t bytes = desc_bytes(total > 0 ? total : 1);
-    if (bytes > c->h_stage_bytes) {
-        if (c->h_stage) GR_CK(cudaFreeHost(c->h_stage));
-        c->h_stage = nullptr;
-        c->h_stage_bytes = 0;
-        if (cudaMallocHost(&c->h_stage, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return GR_ERR_NOMEM;
-        }
-        c->h_stage_bytes = bytes;
+    c->plan.clear();
+    // the descriptor is built on the device (k_plan_nets, k_plan_batches);
+    // only the per-batch totals come back for the launch shapes
+    const size_t bytes = desc_bytes(total > 0 ? total : 1);
+    int rc;
+    if ((rc = ensure(c->plan_desc, bytes, c->stream)) ||
+        (rc = ensure(c->plan_ids, sizeof(int32_t) * (size_t)(total + 1), c->stream)) ||
+        (rc = ensure(c->plan_bofs, sizeof(int64_t) * (size_t)(n_batches + 1), c->stream)) ||
+        (rc = ensure(c->plan_pb, sizeof(PlanBatch) * (size_t)(n_batches + 1) + 16, c->stream)))
+        return rc;
+    uint32_t *d_bad = (uint32_t *)((char *)c->plan_pb.p + sizeof(PlanBatch) * (size_t)(n_batches + 1));
+    if (total > 0)
+        GR_CK(cudaMemcpyAsync(c->plan_ids.p, h_net_ids, sizeof(int32_t) * total, cudaMemcpyHostToDevice, c->stream));
+    GR_CK(cudaMemcpyAsync(c->plan_bofs.p, h_batch_ofs, sizeof(int64_t) * (n_batches + 1), cudaMemcpyHostToDevice,
+                          c->stream));
+    GR_CK(cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), c->stream));
+    const BatchView all = view_of(c->plan_desc.p, total, 0, (int32_t)total);
+    if (total > 0) {
+        k_plan_nets<<<grid_for(c, total), kThreads, 0, c->stream>>>(
+            total, (const int32_t *)c->plan_ids.p, c->n_nets, c->d_pin_ofs, c->d_nxy, const_cast<int64_t *>(all.pin_base),
+            const_cast<int32_t *>(all.npin), const_cast<int32_t *>(all.nxy), d_bad);
+        c->launches++;
     }
-    char *host = (char *)c->h_stage;
+    if (n_batches > 0) {
+        k_plan_batches<<<n_batches, 1024, 0, c->stream>>>(
+            (const int64_t *)c->plan_bofs.p, c->g.Z, kMstWarpPins, kMstMidPins, all.npin, all.nxy,
+            const_cast<int64_t *>(all.pair_ofs), const_cast<int64_t *>(all.node_ofs),
+            const_cast<int64_t *>(all.tab_ofs), const_cast<int32_t *>(all.order), (PlanBatch *)c->plan_pb.p);
+        c->launches++;
+    }
+    GR_CK(cudaGetLastError());
+    std::vector<PlanBatch> pb((size_t)n_batches + 1);
+    uint32_t bad_ids = 0;
+    GR_CK(cudaMemcpyAsync(pb.data(), c->plan_pb.p, sizeof(PlanBatch) * (size_t)n_batches, cudaMemcpyDeviceToHost,
+                          c->stream));
+    GR_CK(cudaMemcpyAsync(&bad_ids, d_bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    GR_CK(cudaStreamSynchronize(c->stream));
+    if (bad_ids) return GR_ERR_ARG;
     std::vector<BatchInfo> plan(n_batches);
     int64_t slot = 0, mp = 0, mt = 0, mn = 0;
-    int bad = 0;
-#pragma omp parallel for schedule(dynamic, 4) reduction(| : bad)
     for (int32_t b = 0; b < n_batches; b++) {
-        int rc = fill_desc(c, h_net_ids + h_batch_ofs[b], (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]), host,
-                           total, h_batch_ofs[b], plan[b]);
-        if (!rc) rc = check_mst_smem(c, plan[b].max_pins);
-        if (rc) bad |= 1 << (-rc);
+        BatchInfo &bi = plan[b];
+        const PlanBatch &q = pb[b];
+        bi.first = h_batch_ofs[b];
+        bi.n = (int32_t)(h_batch_ofs[b + 1] - h_batch_ofs[b]);
+        bi.n_pairs = q.n_pairs;
+        bi.n_nodes = q.n_nodes;
+        bi.n_tab = q.n_tab;
+        bi.max_pins = q.max_pins;
+        bi.n2 = q.n2;
+        bi.nm = q.nm;
+        bi.nmid = q.nmid;
+        bi.nl = bi.n - q.n2 - q.nm;
+        if ((rc = check_mst_smem(c, bi.max_pins))) return rc;
     }
-    if (bad) return (bad & (1 << -GR_ERR_NET_TOO_LARGE)) ? GR_ERR_NET_TOO_LARGE : GR_ERR_ARG;
     for (int32_t b = 0; b < n_batches; b++) {
         plan[b].slot0 = slot;
         slot += plan[b].n_nodes;
@@ -934,14 +1007,10 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
         if (plan[b].n_tab > mt) mt = plan[b].n_tab;
         if (plan[b].n > mn) mn = plan[b].n;
     }
-    int rc;
     int32_t plan_max_pins = 0;
     for (const BatchInfo &bi : plan) plan_max_pins = bi.max_pins > plan_max_pins ? bi.max_pins : plan_max_pins;
     c->plan_max_pins = plan_max_pins;
     if ((rc = ensure_mst_scratch(c, plan_max_pins, c->stream))) return rc;
-    if ((rc = ensure(c->plan_desc, bytes, c->stream))) return rc;
-    GR_CK(cudaMemcpyAsync(c->plan_desc.p, host, bytes, cudaMemcpyHostToDevice, c->stream));
-    GR_CK(cudaEventRecord(c->stage_done, c->stream));
     if ((rc = ensure_scratch(c, mp, mt, mn, c->stream))) return rc;
     GR_CK(cudaStreamSynchronize(c->stream));
     c->plan = std::move(plan);
@@ -954,6 +1023,30 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
 }
 
 int64_t gr_plan_slots(gr_ctx *c) { return c ? c->plan_slots : -1; }
+
+int gr_plan_check(gr_ctx *c) {
+    if (!c) return GR_ERR_ARG;
+    if (c->plan.empty()) return GR_ERR_STATE;
+    int rc = ensure_h_nxy(c);
+    if (rc) return rc;
+    const int64_t total = c->plan_nets;
+    const size_t bytes = desc_bytes(total > 0 ? total : 1);
+    std::vector<int32_t> ids((size_t)total + 1);
+    std::vector<char> dev(bytes), host(bytes, 0);
+    GR_CK(cudaStreamSynchronize(c->stream));
+    if (total > 0)
+        GR_CK(cudaMemcpy(ids.data(), c->plan_ids.p, sizeof(int32_t) * total, cudaMemcpyDeviceToHost));
+    GR_CK(cudaMemcpy(dev.data(), c->plan_desc.p, bytes, cudaMemcpyDeviceToHost));
+    int bad = 0;
+    for (const BatchInfo &bi : c->plan) {
+        BatchInfo hb{};
+        if ((rc = fill_desc(c, ids.data() + bi.first, bi.n, host.data(), total, bi.first, hb))) return rc;
+        bad |= hb.n_pairs != bi.n_pairs || hb.n_nodes != bi.n_nodes || hb.n_tab != bi.n_tab ||
+               hb.max_pins != bi.max_pins || hb.n2 != bi.n2 || hb.nm != bi.nm || hb.nl != bi.nl || hb.nmid != bi.nmid;
+    }
+    bad |= memcmp(dev.data(), host.data(), bytes - 64) != 0;
+    return bad ? GR_ERR_DEVICE : GR_OK;
+}
 
 int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
                   void *stream) {

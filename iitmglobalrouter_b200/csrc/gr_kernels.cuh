@@ -226,6 +226,152 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
     }
 }
 
+// ---------------------------------------------------------------- plan descriptors
+// The SoA descriptor of a whole plan, built on the device from the plan's
+// net ids: per net its pin count, first pin and table shape (k_plan_nets),
+// then per batch (one CTA) the exclusive prefix sums of pairs, MST slots and
+// table entries and the nets' order by size class, batch order kept within
+// a class (k_plan_batches) -- the layout the host builder writes for one
+// batch.
+struct PlanBatch {  // per-batch totals for the host's launch shapes
+    int64_t n_pairs, n_nodes, n_tab;
+    int32_t max_pins, n2, nm, nmid;
+};
+
+__global__ void k_plan_nets(int64_t total, const int32_t *__restrict__ ids, int32_t n_nets,
+                            const int64_t *__restrict__ pin_ofs, const int32_t *__restrict__ nxy_net,
+                            int64_t *__restrict__ pin_base, int32_t *__restrict__ npin, int32_t *__restrict__ nxy,
+                            uint32_t *status) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t id = ids[i];
+        if (id < 0 || id >= n_nets) {
+            atomicOr(status, 1u);
+            id = 0;  // keeps the descriptor in bounds; the host rejects the plan
+        }
+        const int64_t o = pin_ofs[id];
+        pin_base[i] = o;
+        npin[i] = (int32_t)(pin_ofs[id + 1] - o);
+        nxy[i] = nxy_net[id];
+    }
+}
+
+// exclusive prefix of three int64 values over the block (blockDim.x a
+// multiple of 32, at most 1024); totals returned in t0..t2
+__device__ __forceinline__ void block_excl_scan3(int64_t &a, int64_t &b, int64_t &c, int64_t &t0, int64_t &t1,
+                                                 int64_t &t2, int64_t (*wsum)[3]) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int64_t x = a, y = b, z = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t xo = __shfl_up_sync(FULL, x, o), yo = __shfl_up_sync(FULL, y, o), zo = __shfl_up_sync(FULL, z, o);
+        if (lane >= o) x += xo, y += yo, z += zo;
+    }
+    if (lane == 31) wsum[warp][0] = x, wsum[warp][1] = y, wsum[warp][2] = z;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t u = lane < nw ? wsum[lane][0] : 0, v = lane < nw ? wsum[lane][1] : 0, w = lane < nw ? wsum[lane][2] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t uo = __shfl_up_sync(FULL, u, o), vo = __shfl_up_sync(FULL, v, o), wo = __shfl_up_sync(FULL, w, o);
+            if (lane >= o) u += uo, v += vo, w += wo;
+        }
+        if (lane < nw) wsum[lane][0] = u, wsum[lane][1] = v, wsum[lane][2] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const int64_t p0 = warp ? wsum[warp - 1][0] : 0, p1 = warp ? wsum[warp - 1][1] : 0, p2 = warp ? wsum[warp - 1][2] : 0;
+    t0 = wsum[nw - 1][0];
+    t1 = wsum[nw - 1][1];
+    t2 = wsum[nw - 1][2];
+    a = p0 + x - a;
+    b = p1 + y - b;
+    c = p2 + z - c;
+    __syncthreads();  // wsum free for the next call
+}
+
+__global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict__ bofs, int Z, int warp_pins,
+                                                       int mid_pins, const int32_t *__restrict__ npin,
+                                                       const int32_t *__restrict__ nxy, int64_t *__restrict__ pair_ofs,
+                                                       int64_t *__restrict__ node_ofs, int64_t *__restrict__ tab_ofs,
+                                                       int32_t *__restrict__ order, PlanBatch *__restrict__ out) {
+    __shared__ int64_t wsum[32][3];
+    __shared__ int wcnt[4][32];
+    __shared__ int s_max;
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int64_t first = bofs[blockIdx.x];
+    const int n = (int)(bofs[blockIdx.x + 1] - first);
+    auto cls = [&](int k) { return k == 2 ? 0 : (k <= warp_pins ? 1 : (k <= mid_pins ? 2 : 3)); };
+    if (tid == 0) s_max = 0;
+    __syncthreads();
+    // pass 1: offsets, class counts, largest net
+    int64_t P = 0, Mn = 0, T = 0;
+    int c0 = 0, c1 = 0, c2 = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + tid;
+        int64_t a = 0, b = 0, c = 0;
+        int k = 0;
+        if (i < n) {
+            k = npin[first + i];
+            const int q = nxy[first + i];
+            a = (int64_t)k * (k - 1) / 2;
+            b = k;
+            c = (int64_t)Z * (q >> 16) * (q & 0xffff);
+            atomicMax(&s_max, k);
+        }
+        int64_t ta, tb, tc;
+        block_excl_scan3(a, b, c, ta, tb, tc, wsum);
+        if (i < n) {
+            pair_ofs[first + i] = P + a;
+            node_ofs[first + i] = Mn + b;
+            tab_ofs[first + i] = T + c;
+        }
+        P += ta;
+        Mn += tb;
+        T += tc;
+        const int q = i < n ? cls(k) : -1;
+        c0 += __syncthreads_count(q == 0);
+        c1 += __syncthreads_count(q == 1);
+        c2 += __syncthreads_count(q == 2);
+    }
+    // pass 2: stable partition by class
+    int run[4] = {0, c0, c0 + c1, c0 + c1 + c2};
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + tid;
+        const int q = i < n ? cls(npin[first + i]) : -1;
+        unsigned m[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            m[r] = __ballot_sync(FULL, q == r);
+            if (lane == 0) wcnt[r][warp] = __popc(m[r]);
+        }
+        __syncthreads();
+        if (tid < 4) {  // exclusive prefix over the warps, per class
+            int acc = 0;
+            for (int w = 0; w < nw; w++) {
+                const int v = wcnt[tid][w];
+                wcnt[tid][w] = acc;
+                acc += v;
+            }
+        }
+        __syncthreads();
+        if (q >= 0) order[first + run[q] + wcnt[q][warp] + __popc(m[q] & ((1u << lane) - 1))] = i;
+#pragma unroll
+        for (int r = 0; r < 4; r++) run[r] += __syncthreads_count(q == r);
+    }
+    if (tid == 0) {
+        PlanBatch pb;
+        pb.n_pairs = P;
+        pb.n_nodes = Mn;
+        pb.n_tab = T;
+        pb.max_pins = s_max;
+        pb.n2 = c0;
+        pb.nm = c1;
+        pb.nmid = c2;
+        out[blockIdx.x] = pb;
+    }
+}
+
 // ---------------------------------------------------------------- query table
 // Entry (z, a, b) of a net's table: the two prefix queries at (x_a, y_b) on
 // layer z along the layer's direction (x on even layers, y on odd ones).

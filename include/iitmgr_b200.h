@@ -140,6 +140,10 @@ int gr_route_batch(gr_ctx *ctx, const int32_t *h_net_ids, int32_t n_nets, int64_
  * td_net_mst_edges / td_mst_lpat_pat (mst_util.hpp:317-318). */
 int gr_plan_set(gr_ctx *ctx, int32_t n_batches, const int64_t *h_batch_ofs, const int32_t *h_net_ids);
 int64_t gr_plan_slots(gr_ctx *ctx);
+/* Self-check of the uploaded plan (no counterpart in the reference): the
+ * descriptor gr_plan_set built on the device against one built on the host
+ * batch by batch. GR_OK when equal, GR_ERR_DEVICE when not. */
+int gr_plan_check(gr_ctx *ctx);
 #define GR_PLAN_GRAPH 0x1 /* replay the batches as one captured CUDA graph */
 int gr_route_plan(gr_ctx *ctx, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
                   void *stream);

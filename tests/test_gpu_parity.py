@@ -258,6 +258,38 @@ def test_route_persistent_queue_bitexact(cuda, mode):
             assert R.status() == 0
 
 
+def test_plan_descriptor_built_on_device_matches_host_builder(cuda):
+    """gr_plan_set builds the plan's descriptor on the device: equal, array by
+    array and batch total by batch total, to the host builder's, for the
+    generated plans and for a plan with an empty batch and nets of every size
+    class (2, 3..32, 33..128, above 128 pins); ids outside the design are
+    rejected."""
+    L = gr.lib()
+    for config, n_nets in ((1, 0), (2, 30000)):
+        d = gr.Design.generate(config, seed=5, n_nets=n_nets)
+        X, Y, Z, cap, ofs, pins = design_arrays(d)
+        bofs, ids = d.batch(4)
+        R = gr.Router(X, Y, Z, cap)
+        R.set_nets(ofs, pins)
+        R.plan_set(bofs, ids)
+        assert L.gr_plan_check(R._h) == 0
+    X, Y, Z = 40, 40, 4
+    rng = np.random.default_rng(3)
+    sizes = [2, 3, 32, 33, 128, 129, 300, 2, 5, 17, 2, 64, 200] + [int(k) for k in rng.integers(2, 40, 300)]
+    nets = [np.sort(rng.choice(X * Y * 2, size=n, replace=False)).astype(np.int32) for n in sizes]
+    ofs = np.cumsum([0] + sizes).astype(np.int64)
+    R = gr.Router(X, Y, Z, np.ones(X * Y * Z, np.int32))
+    R.set_nets(ofs, np.concatenate(nets))
+    ids = rng.permutation(len(sizes)).astype(np.int32)
+    bofs = np.array([0, 7, 7, 150, len(sizes)], np.int64)  # the second batch is empty
+    R.plan_set(bofs, ids)
+    assert L.gr_plan_check(R._h) == 0
+    bad = ids.copy()
+    bad[100] = len(sizes)
+    with pytest.raises(gr.GRError):
+        R.plan_set(bofs, bad)
+
+
 def test_route_config2_first_batches_bitexact(cuda):
     """The 400x400x9 design (odd Z), first batches of the -batch_part plan."""
     d = gr.Design.generate(2, seed=1, n_nets=40000)
