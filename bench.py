@@ -384,8 +384,12 @@ def main():
             e2e_times.append(t1 - t0)
     e2e_t = replicas.max_over_ranks(statistics.median(e2e_times), dist, dev)
     assert np.array_equal(h_mst.numpy(), mst_h), "end-to-end result differs from the resident run"
-    h2d = pins.nbytes + (ids.size * 36 + 64)  # design pins + plan descriptor (pin offsets stay on the host)
-    d2h = M * 8 + M * 4
+    # uploads: pins, pin offsets, the list of nets above 32 pins, the plan's net ids and batch offsets
+    # (the plan descriptor itself is built on the device); downloads: trees and patterns, plus
+    # the per-batch totals of the plan (40 B a batch)
+    npin = np.diff(ofs)
+    h2d = pins.nbytes + ofs.nbytes + 4 * int((npin > 32).sum()) + ids.nbytes + bofs.nbytes
+    d2h = M * 8 + M * 4 + 40 * (len(bofs) - 1)
 
     cpu = None
     if rank == 0:
