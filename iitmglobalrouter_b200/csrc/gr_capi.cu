@@ -125,6 +125,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMstSmemMax = 200 * 1024;  // dynamic shared memory of k_mst_large
+constexpr int kFenTrackMaxL = 3072;      // longest track k_fen_tracks stages (4 warps x 2 x L floats = 96 KB)
 constexpr int kMstMidPins = 128;         // k_mst_large on 128 threads up to this size
 constexpr int kMstClusterSmem = 216 * 1024;  // dynamic shared memory of k_mst_cluster CTAs
 
@@ -588,7 +589,11 @@ void drop_graph(gr_ctx *c) {
 // Fenwick trees from the current capacities, with the plain or the lookahead cost
 int rebuild_fenwick(gr_ctx *c, cudaStream_t s) {
     int pi = prof_begin(c, s);
-    if (c->la_on)
+    const int lmax = c->g.X > c->g.Y ? c->g.X : c->g.Y;
+    if (lmax <= kFenTrackMaxL)  // a warp per track, the track staged in shared memory
+        k_fen_tracks<<<(c->n_tracks + 3) / 4, 128, (size_t)4 * 2 * lmax * sizeof(float), s>>>(
+            c->g, (int)c->n_tracks, c->la_on ? 1 : 0, c->d_capr, c->d_lut, c->d_pred, c->la_beta, c->d_fen);
+    else if (c->la_on)
         k_fen_init_la<<<grid_for(c, c->csize, 16), kThreads, 0, s>>>(c->g, (int)c->csize, c->d_capr, c->d_pred,
                                                                      c->la_beta, c->d_fen);
     else
@@ -714,7 +719,9 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         return fail(GR_ERR_CUDA);
     if (cudaFuncSetAttribute(k_mst_large, cudaFuncAttributeMaxDynamicSharedMemorySize, c->mst_smem_max) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(k_mst_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstSmemMax) != cudaSuccess)
+        cudaFuncSetAttribute(k_mst_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, kMstSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(k_fen_tracks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             4 * 2 * kFenTrackMaxL * (int)sizeof(float)) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     if ((rc = gr_reset(c, nullptr))) return fail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(GR_ERR_CUDA);

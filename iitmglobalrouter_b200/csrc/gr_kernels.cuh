@@ -226,6 +226,50 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
     }
 }
 
+// Routing tracks (a row of an even layer, a column of an odd layer) are
+// numbered layer by layer: layer z starts at track_first(z).
+__device__ __forceinline__ int track_first(const GridC &g, int z) { return ((z + 1) >> 1) * g.Y + (z >> 1) * g.X; }
+
+// The same, one warp per routing track (a row of an even layer, a column of
+// an odd one; tracks numbered layer by layer from track_first): the track's
+// cell costs are staged in shared memory, then the nodes are built level by
+// level -- node i (lowbit 2^k) is its left half's node i - 2^(k-1) followed
+// by the cells of its right half added one by one in ascending order, the
+// same left-to-right sequence of FP32 additions as summing its whole range
+// from 0, so every node is bit-identical to k_fen_init's. Shared memory per
+// warp: 2 * L floats (costs, nodes); la != 0 uses the lookahead cost.
+__global__ void __launch_bounds__(128) k_fen_tracks(GridC g, int n_tracks, int la, const int32_t *__restrict__ capr,
+                                                    const float *__restrict__ lut, const float *__restrict__ pred,
+                                                    float beta, float *__restrict__ fen) {
+    extern __shared__ float fsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int Lmax = g.X > g.Y ? g.X : g.Y;
+    float *cst = fsm + (size_t)wib * 2 * Lmax, *node = cst + Lmax;
+    const int t = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (t >= n_tracks) return;
+    int z = 0;
+    while (z + 1 < g.Z && track_first(g, z + 1) <= t) z++;
+    const int r = t - track_first(g, z);
+    const int L = (z & 1) ? g.Y : g.X;
+    const int32_t base = z * g.XY + r * L;
+    for (int q = lane; q < L; q += 32) {
+        const int32_t e = base + q;
+        cst[q] = la ? la_cost(__ldg(capr + e), __ldg(pred + e), beta) : lut_cost(lut, __ldg(capr + e));
+    }
+    __syncwarp();
+    for (int i = 1 + 2 * lane; i <= L; i += 64) node[i - 1] = 0.0f + cst[i - 1];  // lowbit 1
+    __syncwarp();
+    for (int h = 1; 2 * h <= L; h <<= 1) {  // lowbit 2h: i = 2h (2j + 1)
+        for (int i = 2 * h * (2 * lane + 1); i <= L; i += 2 * h * 64) {
+            float v = node[i - h - 1];
+            for (int q = i - h + 1; q <= i; q++) v += cst[q - 1];
+            node[i - 1] = v;
+        }
+        __syncwarp();
+    }
+    for (int q = lane; q < L; q += 32) fen[base + q] = node[q];
+}
+
 // ---------------------------------------------------------------- plan descriptors
 // The SoA descriptor of a whole plan, built on the device from the plan's
 // net ids: per net its pin count, first pin and table shape (k_plan_nets),
@@ -1303,9 +1347,6 @@ struct PathUnits {
 
 
 // ---------------------------------------------------------------- commit by track
-// Routing tracks (a row of an even layer, a column of an odd layer) are
-// numbered layer by layer: layer z starts at track_first(z).
-__device__ __forceinline__ int track_first(const GridC &g, int z) { return ((z + 1) >> 1) * g.Y + (z >> 1) * g.X; }
 
 // track index and first cell of the track holding cell e
 __device__ __forceinline__ void track_of(const GridC &g, int32_t e, int &t, int32_t &base) {

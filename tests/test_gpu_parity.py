@@ -258,6 +258,19 @@ def test_route_persistent_queue_bitexact(cuda, mode):
             assert R.status() == 0
 
 
+@pytest.mark.parametrize("X,Y,Z", [(37, 53, 5), (64, 64, 4), (3100, 6, 3)])
+def test_fenwick_build_bitexact(cuda, X, Y, Z):
+    """The Fenwick trees of a reset (one warp per track, levels built from
+    their left halves; the per-cell kernel for tracks above 3072 cells)
+    equal the oracle's bit for bit."""
+    rng = np.random.default_rng(X * Y + Z)
+    cap = rng.integers(-3, 40, size=X * Y * Z).astype(np.int32)
+    R = gr.Router(X, Y, Z, cap)
+    R.reset()
+    g = oracle.Grid(X, Y, Z, cap)
+    assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))
+
+
 def test_plan_descriptor_built_on_device_matches_host_builder(cuda):
     """gr_plan_set builds the plan's descriptor on the device: equal, array by
     array and batch total by batch total, to the host builder's, for the
