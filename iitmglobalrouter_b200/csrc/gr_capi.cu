@@ -107,6 +107,7 @@ struct gr_ctx {
     int mst_smem_max = 0;
     int32_t plan_max_pins = 0;  // largest net of the uploaded plan
     DevBuf plan_ids, plan_bofs, plan_pb;  // device plan builder: inputs, per-batch totals and an error flag
+    DevBuf plan_slot0, slot_net;          // per batch its first MST slot; per plan slot its net
     bool h_nxy_valid = false;             // h_nxy mirrors d_nxy (copied when a host-built descriptor needs it)
     int *d_queue = nullptr;  // k_mst_queue: next item, CTAs finished (zero between launches)
     int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
@@ -773,6 +774,8 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->plan_ids);
     free_buf(c->plan_bofs);
     free_buf(c->plan_pb);
+    free_buf(c->plan_slot0);
+    free_buf(c->slot_net);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -1019,6 +1022,20 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     c->plan_max_pins = plan_max_pins;
     if ((rc = ensure_mst_scratch(c, plan_max_pins, c->stream))) return rc;
     if ((rc = ensure_scratch(c, mp, mt, mn, c->stream))) return rc;
+    // slot -> net map for the marking kernel (saves it a search per slot)
+    if (n_batches > 0 && slot > 0) {
+        std::vector<int64_t> s0(n_batches);
+        for (int32_t b = 0; b < n_batches; b++) s0[b] = plan[b].slot0;
+        if ((rc = ensure(c->plan_slot0, sizeof(int64_t) * n_batches, c->stream)) ||
+            (rc = ensure(c->slot_net, sizeof(int32_t) * (size_t)slot, c->stream)))
+            return rc;
+        GR_CK(cudaMemcpyAsync(c->plan_slot0.p, s0.data(), sizeof(int64_t) * n_batches, cudaMemcpyHostToDevice,
+                              c->stream));
+        k_plan_slots<<<n_batches, 256, 0, c->stream>>>((const int64_t *)c->plan_bofs.p, (const int64_t *)c->plan_slot0.p,
+                                                      all.npin, all.node_ofs, (int32_t *)c->slot_net.p);
+        c->launches++;
+        GR_CK(cudaGetLastError());
+    }
     GR_CK(cudaStreamSynchronize(c->stream));
     c->plan = std::move(plan);
     c->plan_nets = total;
@@ -1070,6 +1087,7 @@ int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32
         for (int32_t b = b0; b < b1; b++) {
             const BatchInfo &bi = c->plan[b];
             BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
+            if (c->slot_net.p) v.slot_net = (const int32_t *)c->slot_net.p + bi.slot0;
             int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr,
                                (float *)c->dist.p, (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
             if (rc) return rc;

@@ -40,6 +40,7 @@ struct BatchView {
     int32_t max_pins;
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
     int32_t nmid;             // of the nl larger nets, the first nmid have at most 128 pins
+    const int32_t *slot_net;  // [n_nodes] net of each MST slot (plans only; null: found by search)
 };
 
 // Per design pin (indexed like the pin array): the pin's index into its net's
@@ -223,6 +224,20 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
         float res = 0.0f;
         for (int q = lo; q <= i; q++) res += lut_cost(lut, __ldg(capr + base + q - 1));
         fen[e] = res;
+    }
+}
+
+// The plan's slot -> net map: slot slot0[b] + node_ofs[i] + j (pin j of net i
+// of batch b) holds i. One CTA per batch, one thread per net.
+__global__ void k_plan_slots(const int64_t *__restrict__ bofs, const int64_t *__restrict__ slot0,
+                             const int32_t *__restrict__ npin, const int64_t *__restrict__ node_ofs,
+                             int32_t *__restrict__ slot_net) {
+    const int64_t first = bofs[blockIdx.x];
+    const int n = (int)(bofs[blockIdx.x + 1] - first);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int32_t *dst = slot_net + slot0[blockIdx.x] + node_ofs[first + i];
+        const int k = npin[first + i];
+        for (int j = 0; j < k; j++) dst[j] = i;
     }
 }
 
@@ -1374,7 +1389,7 @@ __global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int3
     PathUnits &pu = su[wib];
     for (int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; s < bv.n_nodes; s += nwarps) {
         int units = 0;
-        const int net = warp_ofs_search(bv.node_ofs, bv.n, s, lane);
+        const int net = bv.slot_net ? __ldg(bv.slot_net + s) : warp_ofs_search(bv.node_ofs, bv.n, s, lane);
         if (lane == 0) {
             pu.seg_n = 0;
             pu.seg_u[0] = 0;
