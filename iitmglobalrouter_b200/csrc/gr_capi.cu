@@ -479,10 +479,11 @@ constexpr int kTrackCapMax = 1024;   // marked cells per track kept in shared me
 
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
 
+// count_cleared: an L-pattern kernel of this batch already set the track count to 0
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool count_cleared = false) {
     if (v.n_nodes <= 0) return GR_OK;
-    GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
+    if (!count_cleared) GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
     int pi = prof_begin(c, s);
     k_mark7<<<grid_for(c, v.n_nodes * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
                                                                 c->d_tbits, c->d_tlist, c->d_list_count,
@@ -571,9 +572,11 @@ int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchV
 int route_one(gr_ctx *c, const BatchView &v, int64_t *mst, int32_t *mst_pat, float *dist, float *pcost,
               int16_t *ppat, cudaStream_t s) {
     int rc;
-    if ((rc = launch_lpat_batch(c, v, pcost, ppat, (float2 *)c->tab.p, s, mst, dist))) return rc;
+    BatchView vl = v;  // the L-pattern kernel also clears the marking's track count
+    vl.zero_count = c->d_list_count;
+    if ((rc = launch_lpat_batch(c, vl, pcost, ppat, (float2 *)c->tab.p, s, mst, dist))) return rc;
     if ((rc = launch_mst(c, v, pcost, mst, dist, s, true))) return rc;
-    return launch_commit(c, v, mst, ppat, mst_pat, s);
+    return launch_commit(c, v, mst, ppat, mst_pat, s, v.n_pairs > 0);
 }
 
 void free_buf(DevBuf &b) {

@@ -41,7 +41,14 @@ struct BatchView {
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
     int32_t nmid;             // of the nl larger nets, the first nmid have at most 128 pins
     const int32_t *slot_net;  // [n_nodes] net of each MST slot (plans only; null: found by search)
+    int32_t *zero_count;      // set to 0 by the L-pattern kernel (the marking's track count), or null
 };
+
+// the L-pattern kernels clear the batch's touched-track count for the marking
+// kernel that follows them (one memset node less per batch)
+__device__ __forceinline__ void lpat_clear_count(const BatchView &bv) {
+    if (bv.zero_count && blockIdx.x == 0 && threadIdx.x == 0) *bv.zero_count = 0;
+}
 
 // Per design pin (indexed like the pin array): the pin's index into its net's
 // sorted distinct x and y lists, packed (xi << 16) | yi; and the lists
@@ -476,6 +483,7 @@ __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const
                                                     const float2 *__restrict__ tab,
                                                     float *__restrict__ cost, int16_t *__restrict__ pat,
                                                     int64_t *__restrict__ mst, float *__restrict__ dist) {
+    lpat_clear_count(bv);
     const int lane = threadIdx.x & 31;
     for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
          p0 += (int64_t)gridDim.x * blockDim.x) {
@@ -967,6 +975,7 @@ __global__ void __launch_bounds__(256, 2) k_lpat_z(GridC g, BatchView bv, const 
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
                                                 float *__restrict__ cost, int16_t *__restrict__ pat,
                                                 int64_t *__restrict__ mst, float *__restrict__ dist) {
+    lpat_clear_count(bv);
     const int lane = threadIdx.x & 31;
     for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
          p0 += (int64_t)gridDim.x * blockDim.x) {
@@ -1017,6 +1026,7 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
                                                  const float2 *__restrict__ tab, float *__restrict__ cost,
                                                  int16_t *__restrict__ pat, int64_t *__restrict__ mst,
                                                  float *__restrict__ dist) {
+    lpat_clear_count(bv);
     static_assert(S == 2 || S == 4 || S == 8, "warps per pair group");
     __shared__ float sc[8][32];
     __shared__ int sp[8][32], sf[8][32];
