@@ -49,10 +49,26 @@ __device__ __forceinline__ int32_t track_base(const GridC &g, int z, int x, int 
 }
 
 // Inclusive prefix query of one track (bit_util.hpp:19-35): nodes from
-// index pos+1 down to 1, accumulated in that order starting from 0.
+// index pos+1 down to 1, accumulated in that order starting from 0. The
+// node indices depend on pos alone, so up to eight nodes are loaded before
+// any is added (the loads overlap instead of each waiting for the previous
+// addition); the additions keep the reference's order.
 __device__ __forceinline__ float fen_query(const float *__restrict__ fen, int32_t base, int pos) {
     float res = 0.0f;
-    for (int i = pos + 1; i > 0; i &= i - 1) res += __ldg(fen + base + i - 1);
+    int i = pos + 1;
+    while (i > 0) {
+        float v[8];
+        bool on[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            on[k] = i > 0;
+            v[k] = on[k] ? __ldg(fen + base + i - 1) : 0.0f;
+            i &= i - 1;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (on[k]) res += v[k];
+    }
     return res;
 }
 
