@@ -111,23 +111,27 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
 }
 
 // ------------------------------------------------------------------ forward convolution on tcgen05
-// One CTA computes 128 positions x Nt (16 or 32) output channels of a layer
-// as an implicit GEMM: the 128 x Kp patch matrix is gathered from the input
-// (fp32 -> bf16, zero outside the grid) straight into shared memory in the
+// One CTA computes a tile of 8 x 16 positions (128) x Nt (16 or 32) output
+// channels of a layer as an implicit GEMM. The tile's input with its one-cell
+// halo, 10 x 18 cells of every channel (rounded up to a multiple of 8
+// channels), is loaded once into shared memory as bf16 (zero outside the
+// grid); the 128 x Kp patch matrix is built from it in shared memory in the
 // canonical K-major layout without swizzle (8-row x 16-byte core matrices;
 // core matrix (row group g, k chunk c) at c * LBO + g * 128 bytes), the
 // weights likewise as an Nt x Kp matrix; one thread issues the Kp / 16
 // tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator of 128 lanes x Nt
 // columns in tensor memory) and commits them to an mbarrier; the epilogue
 // reads the accumulator with tcgen05.ld (warp w: lanes 32 (w % 4) .., columns
-// 16 (w / 4) ..), adds the bias, applies ReLU and writes Y[n][m] (coalesced
-// over m) and, when training, the pre-activation Z[m][n].
+// 16 (w / 4) ..), adds the bias, applies ReLU and writes Y[n][y][x] (rows of
+// 16 positions) and, when training, the pre-activation Z[m][n].
 constexpr int kConvThreads = 256, kConvRows = 128, kConvTmemCols = 32;
+constexpr int kConvTY = 8, kConvTX = 16, kHaloY = kConvTY + 2, kHaloX = kConvTX + 2, kHalo = kHaloY * kHaloX;
 constexpr int kConvSmemMax = 200 * 1024;
 constexpr long long kConvWaitLimit = 1ll << 24;  // mbarrier polls before the kernel reports a stall
 
-__host__ __device__ constexpr int conv_smem_bytes(int Kp, int Nt) {
-    return 1024 + kConvRows * Kp * 2 + Nt * Kp * 2 + 64;
+__host__ __device__ constexpr int conv_halo_bytes(int cin) { return ((cin + 7) / 8) * 8 * kHalo * 2; }
+__host__ __device__ constexpr int conv_smem_bytes(int Kp, int Nt, int cin) {
+    return 1024 + kConvRows * Kp * 2 + Nt * Kp * 2 + conv_halo_bytes(cin) + 64;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -182,10 +186,11 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     uint8_t *base = (uint8_t *)(((uintptr_t)conv_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *As = base;                                   // 128 x Kp
     uint8_t *Bs = As + kConvRows * Kp * 2;                // Nt x Kp
-    uint64_t *bar = (uint64_t *)(Bs + Nt * Kp * 2);       // 8-byte aligned (Kp multiple of 16)
+    __nv_bfloat16 *halo = (__nv_bfloat16 *)(Bs + Nt * Kp * 2);  // [channel][10][18]
+    uint64_t *bar = (uint64_t *)((uint8_t *)halo + conv_halo_bytes(cin));  // 8-byte aligned
     uint32_t *tmem_slot = (uint32_t *)(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int M = H * W, m0 = blockIdx.x * kConvRows;
+    const int M = H * W, y0 = blockIdx.y * kConvTY, x0 = blockIdx.x * kConvTX;
     const int nchunk = Kp >> 3;
 
     if (warp == 0) {
@@ -214,40 +219,44 @@ __global__ void __launch_bounds__(kConvThreads, 2)
         *(uint4 *)(Bs + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 
-    // patches: thread (row r, half h) fills the channel groups g = h, h + 2, ...
-    // of row r. A group of 8 channels is 72 k values = 9 whole chunks, so the
-    // fully unrolled loop has every element's channel, tap and word position
-    // fixed at compile time; a tap outside the grid, a row past M and a
-    // channel past cin read as zero, and chunks past Kp are not stored.
+    // the halo tile: rows y0 - 1 .. y0 + 8, columns x0 - 1 .. x0 + 16, channels
+    // up to the next multiple of 8 (the extra ones zero)
+    const int ngroups = (cin + 7) >> 3;
+    const int nhalo = ngroups * 8 * kHalo;
+    for (int i0 = tid; i0 < nhalo; i0 += 8 * kConvThreads) {  // eight loads in flight per thread
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = i0 + u * kConvThreads;
+            const int ci = i / kHalo, rem = i - ci * kHalo, hy = rem / kHaloX, hx = rem - hy * kHaloX;
+            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
+            v[u] = (i < nhalo && ci < cin && gy >= 0 && gy < H && gx >= 0 && gx < W)
+                       ? __ldg(X + (long long)ci * M + gy * W + gx)
+                       : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (i0 + u * kConvThreads < nhalo) halo[i0 + u * kConvThreads] = __float2bfloat16(v[u]);
+    }
+    __syncthreads();
+    // patches: thread (row r = ty * 16 + tx, half h) fills the channel groups
+    // g = h, h + 2, ... of row r from the halo. A group of 8 channels is 72 k
+    // values = 9 whole chunks, so every element's halo offset and word
+    // position are compile-time constants; chunks past Kp are not stored.
     {
         const int r = tid & (kConvRows - 1), h = tid >> 7;
-        const int m = m0 + r;
-        const int y = m < M ? m / W : 0, x = m < M ? m - y * W : 0;
-        int vmask = 0;  // bit t = dy * 3 + dx: tap inside the grid
-        int off[9];
-#pragma unroll
-        for (int t = 0; t < 9; t++) {
-            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
-            vmask |= (m < M && yy >= 0 && yy < H && xx >= 0 && xx < W) << t;
-            off[t] = (t / 3 - 1) * W + (t % 3 - 1);
-        }
-        const int ngroups = (cin + 7) >> 3;
+        const int ty = r / kConvTX, tx = r - ty * kConvTX;
+        const uint16_t *hrow = reinterpret_cast<const uint16_t *>(halo) + ty * kHaloX + tx;
         uint8_t *arow = As + r * 16;
         for (int gi = h; gi < ngroups; gi += 2) {
-            const float *base = X + (long long)(gi * 8) * M + m;
-            const int nch = cin - gi * 8;  // channels of this group that exist (may exceed 8)
+            const uint16_t *hg = hrow + gi * 8 * kHalo;
             uint32_t w[4];
 #pragma unroll
             for (int e = 0; e < 72; e += 2) {
-                float v[2];
-#pragma unroll
-                for (int u = 0; u < 2; u++) {
-                    const int j = (e + u) / 9, t = (e + u) % 9;
-                    const bool ok = j < nch && ((vmask >> t) & 1);
-                    v[u] = ok ? __ldg(base + (long long)j * M + off[t]) : 0.0f;
-                }
-                const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[0], v[1]);
-                w[(e >> 1) & 3] = *reinterpret_cast<const uint32_t *>(&b2);
+                const int j0 = e / 9, t0 = e % 9, j1 = (e + 1) / 9, t1 = (e + 1) % 9;
+                const uint32_t lo = hg[j0 * kHalo + (t0 / 3) * kHaloX + t0 % 3];
+                const uint32_t hi = hg[j1 * kHalo + (t1 / 3) * kHaloX + t1 % 3];
+                w[(e >> 1) & 3] = lo | (hi << 16);
                 if (((e >> 1) & 3) == 3) {
                     const int c = gi * 9 + (e >> 3);
                     if (c < nchunk)
@@ -292,8 +301,9 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     if (done && 16 * half < Nt) {
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * half, v);
-        const int m = m0 + 32 * q + lane;
-        if (m < M) {
+        const int r = 32 * q + lane, yy = y0 + r / kConvTX, xx = x0 + r % kConvTX;
+        const int m = yy * W + xx;
+        if (yy < H && xx < W) {
 #pragma unroll
             for (int j = 0; j < 16; j++) {
                 const int n = 16 * half + j;
@@ -625,9 +635,12 @@ int pack_all(gr_cnn *c) {
     return GR_OK;
 }
 
+// tiles of 16 columns x 8 rows
+dim3 conv_grid(const gr_cnn *c) { return dim3((c->W + kConvTX - 1) / kConvTX, (c->H + kConvTY - 1) / kConvTY); }
+
 // the tensor-core convolution takes a layer whose tiles fit in shared memory
 bool conv_tc_fits(const gr_cnn *c, int l) {
-    return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16)) <= kConvSmemMax;
+    return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16), c->cin[l]) <= kConvSmemMax;
 }
 
 int forward(gr_cnn *c) {
@@ -637,7 +650,7 @@ int forward(gr_cnn *c) {
         const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
         if (conv_tc_fits(c, l)) {
             const int Nt = round_up(c->cout[l], 16);
-            k_conv_tc<<<(M + kConvRows - 1) / kConvRows, kConvThreads, conv_smem_bytes(c->Kp[l], Nt), s>>>(
+            k_conv_tc<<<conv_grid(c), kConvThreads, conv_smem_bytes(c->Kp[l], Nt, c->cin[l]), s>>>(
                 c->cin[l], c->cout[l], c->H, c->W, c->Kp[l], Nt, c->Np[l], c->act[l], c->wt[l], bl, c->act[l + 1],
                 nullptr, l + 1 < c->n_layers, c->err);
             continue;
@@ -671,8 +684,7 @@ int backward(gr_cnn *c, const float *d_target) {
         k_wgrad_tc<<<dim3(splits, ktiles), kConvThreads, wgrad_smem_bytes(Nt), s>>>(cin, co, c->H, c->W, Nt, per,
                                                                                    c->act[l], dY, g, c->err);
         if (l > 0) {  // cin = hidden <= 32 and cout <= 32: always within the tensor-core tile
-            k_conv_tc<<<(M + kConvRows - 1) / kConvRows, kConvThreads, conv_smem_bytes(c->KpT[l], round_up(cin, 16)),
-                        s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
+            k_conv_tc<<<conv_grid(c), kConvThreads, conv_smem_bytes(c->KpT[l], round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
                              dX, nullptr, 0, c->err);
             float *t = dY;
             dY = dX;
