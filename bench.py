@@ -378,7 +378,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         R.route_design_host(h_ofs.numpy(), h_pins.numpy(), h_bofs.numpy(), h_ids.numpy(), h_mst.numpy(),
-                            h_pat.numpy())
+                            h_pat.numpy(), graph=True)
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e_times.append(t1 - t0)

@@ -44,9 +44,7 @@ struct BatchInfo {  // one batch of a plan
 
 struct GraphCache {
     cudaGraphExec_t exec = nullptr;
-    int32_t b0 = -1, b1 = -1;
-    void *mst = nullptr, *pat = nullptr;
-    cudaStream_t stream = nullptr;
+    std::vector<uint64_t> sig;  // everything the captured launches and copies were built from
     int64_t launches = 0;
 };
 
@@ -79,6 +77,7 @@ struct gr_ctx {
     DevBuf la_feat, la_out;              // network input and output of the lookahead route
     cudaStream_t copy_stream = nullptr;  // its result copies, overlapping the route
     cudaEvent_t ev_out = nullptr;
+    cudaEvent_t ev_copy_done = nullptr;  // result copies joined back to the route's stream
     void *h_stage = nullptr;
     size_t h_stage_bytes = 0;
     cudaEvent_t stage_done = nullptr;
@@ -663,7 +662,8 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
         return fail(GR_ERR_CUDA);
     if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess) return fail(GR_ERR_CUDA);
     if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_copy_done, cudaEventDisableTiming) != cudaSuccess)
         return fail(GR_ERR_CUDA);
     for (int i = 0; i < 3; i++)
         if (cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking) != cudaSuccess ||
@@ -770,6 +770,7 @@ int gr_destroy(gr_ctx *c) {
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream), cudaStreamDestroy(c->copy_stream);
     if (c->ev_out) cudaEventDestroy(c->ev_out);
+    if (c->ev_copy_done) cudaEventDestroy(c->ev_copy_done);
     free_buf(c->out_mst);
     free_buf(c->out_pat);
     free_buf(c->la_feat);
@@ -818,7 +819,8 @@ int gr_set_nets(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32
     for (int64_t t = 0; t < total; t++) bad_pin |= h_pins[t] < 0 || h_pins[t] >= csize;
     if (bad_pin) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
-    drop_graph(c);
+    // a captured plan stays: it is replayed only if its signature (buffer
+    // addresses, batch shapes) still matches (graph_sig)
     if ((size_t)(total + 1) > c->pins_cap) {
         for (int32_t **p : {&c->d_pins, &c->d_pxy, &c->d_cx, &c->d_cy}) {
             if (*p) cudaFree(*p);
@@ -957,8 +959,7 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     for (int32_t b = 0; b < n_batches; b++)
         if (h_batch_ofs[b + 1] < h_batch_ofs[b]) return GR_ERR_ARG;
     GR_CK(cudaStreamSynchronize(c->stream));
-    drop_graph(c);
-    c->plan.clear();
+    c->plan.clear();  // a captured plan is replayed only if its signature still matches
     // the descriptor is built on the device (k_plan_nets, k_plan_batches);
     // only the per-batch totals come back for the launch shapes
     const size_t bytes = desc_bytes(total > 0 ? total : 1);
@@ -1075,17 +1076,51 @@ int gr_plan_check(gr_ctx *c) {
     return bad ? GR_ERR_DEVICE : GR_OK;
 }
 
-int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
-                  void *stream) {
-    if (!c || !d_mst_edges || b0 < 0 || b1 < b0 || b1 > (int32_t)c->plan.size()) return GR_ERR_ARG;
-    if (c->plan.empty() && b1 > 0) return GR_ERR_STATE;
-    cudaStream_t s = pick(c, stream);
+}  // extern "C"
+
+namespace {
+
+// What a captured plan depends on beyond the contents of device memory: the
+// batches' launch shapes and offsets, every buffer address its launches and
+// copies use, the launch-shape parameters and the cost mode. A graph is
+// replayed only while all of it is unchanged.
+std::vector<uint64_t> graph_sig(const gr_ctx *c, int32_t b0, int32_t b1, const void *mst, const void *pat,
+                                cudaStream_t s, const void *h_mst, const void *h_pat) {
+    std::vector<uint64_t> v;
+    auto P = [&](const void *p) { v.push_back((uint64_t)(uintptr_t)p); };
+    const void *const ptrs[] = {mst, pat, (const void *)s, h_mst, h_pat, c->plan_desc.p, c->slot_net.p, c->pcost.p,
+                          c->ppat.p, c->tab.p, c->dist.p, c->mat.p, (const void *)c->d_pins, (const void *)c->d_pxy,
+                          (const void *)c->d_cx, (const void *)c->d_cy, (const void *)c->d_fen, (const void *)c->d_capr,
+                          (const void *)c->d_mark, (const void *)c->d_tbits, (const void *)c->d_tlist,
+                          (const void *)c->d_list_count, (const void *)c->d_status, (const void *)c->d_dlut,
+                          (const void *)c->d_gpos, (const void *)c->d_gdel, (const void *)c->d_pred,
+                          (const void *)c->d_queue};
+    for (const void *p : ptrs) P(p);
+    v.push_back((uint64_t)b0 << 32 | (uint32_t)b1);
+    v.push_back((uint64_t)c->plan_nets);
+    for (int t = 0; t < GR_TUNE_PARAMS; t++) v.push_back((uint64_t)(uint32_t)c->tune[t]);
+    uint32_t beta_bits;
+    memcpy(&beta_bits, &c->la_beta, 4);
+    v.push_back((uint64_t)c->la_on << 32 | beta_bits);
+    for (int32_t b = b0; b < b1; b++) {
+        const BatchInfo &bi = c->plan[b];
+        const int64_t f[] = {bi.first, (int64_t)bi.n, bi.n_pairs, bi.n_nodes, bi.n_tab, bi.slot0, (int64_t)bi.max_pins,
+                             (int64_t)bi.n2, (int64_t)bi.nm, (int64_t)bi.nl, (int64_t)bi.nmid};
+        for (int64_t x : f) v.push_back((uint64_t)x);
+    }
+    return v;
+}
+
+// gr_route_plan, optionally with the results copied to page-locked host
+// buffers chunk by chunk on the copy stream while later chunks route (the
+// copies are part of the graph when one is captured)
+int route_plan_impl(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
+                    cudaStream_t s, int64_t *h_mst, int32_t *h_pat) {
     // the Boruvka scratch depends on the launch shapes, which may have changed
-    // since gr_plan_set (a captured graph holds the scratch's address)
-    const void *mat_before = c->mat.p;
+    // since gr_plan_set
     int rc0 = ensure_mst_scratch(c, c->plan_max_pins, s);
     if (rc0) return rc0;
-    if (c->mat.p != mat_before) drop_graph(c);
+    const int32_t chunk = 32;
     auto issue = [&]() -> int {
         for (int32_t b = b0; b < b1; b++) {
             const BatchInfo &bi = c->plan[b];
@@ -1094,13 +1129,29 @@ int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32
             int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr,
                                (float *)c->dist.p, (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
             if (rc) return rc;
+            if (h_mst && ((b + 1 - b0) % chunk == 0 || b + 1 == b1)) {
+                const int32_t c0 = b + 1 - ((b + 1 - b0) % chunk ? (b + 1 - b0) % chunk : chunk);
+                const int64_t s0 = c->plan[c0].slot0, s1 = b + 1 < (int32_t)c->plan.size() ? c->plan[b + 1].slot0
+                                                                                             : c->plan_slots;
+                GR_CK(cudaEventRecord(c->ev_out, s));
+                GR_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_out, 0));
+                GR_CK(cudaMemcpyAsync(h_mst + s0, d_mst_edges + s0, sizeof(int64_t) * (s1 - s0),
+                                      cudaMemcpyDeviceToHost, c->copy_stream));
+                if (h_pat)
+                    GR_CK(cudaMemcpyAsync(h_pat + s0, d_mst_pat + s0, sizeof(int32_t) * (s1 - s0),
+                                          cudaMemcpyDeviceToHost, c->copy_stream));
+            }
+        }
+        if (h_mst) {  // the copy stream joins back
+            GR_CK(cudaEventRecord(c->ev_copy_done, c->copy_stream));
+            GR_CK(cudaStreamWaitEvent(s, c->ev_copy_done, 0));
         }
         return GR_OK;
     };
     if (!(flags & GR_PLAN_GRAPH)) return issue();
     GraphCache &gc = c->graph;
-    if (!(gc.exec && gc.b0 == b0 && gc.b1 == b1 && gc.mst == d_mst_edges && gc.pat == d_mst_pat &&
-          gc.stream == s)) {
+    std::vector<uint64_t> sig = graph_sig(c, b0, b1, d_mst_edges, d_mst_pat, s, h_mst, h_pat);
+    if (!(gc.exec && gc.sig == sig)) {
         drop_graph(c);
         int64_t before = c->launches;
         cudaGraph_t graph = nullptr;
@@ -1118,17 +1169,24 @@ int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32
             gc.exec = nullptr;
             return GR_ERR_CUDA;
         }
-        gc.b0 = b0;
-        gc.b1 = b1;
-        gc.mst = d_mst_edges;
-        gc.pat = d_mst_pat;
-        gc.stream = s;
+        gc.sig = std::move(sig);
         gc.launches = c->launches - before;
         c->launches = before;
     }
     GR_CK(cudaGraphLaunch(gc.exec, s));
     c->launches += gc.launches;
     return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gr_route_plan(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int32_t *d_mst_pat, int flags,
+                  void *stream) {
+    if (!c || !d_mst_edges || b0 < 0 || b1 < b0 || b1 > (int32_t)c->plan.size()) return GR_ERR_ARG;
+    if (c->plan.empty() && b1 > 0) return GR_ERR_STATE;
+    return route_plan_impl(c, b0, b1, d_mst_edges, d_mst_pat, flags, pick(c, stream), nullptr, nullptr);
 }
 
 int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, const int32_t *h_pins,
@@ -1146,7 +1204,7 @@ int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, co
     int64_t *mst = (int64_t *)c->out_mst.p;
     int32_t *pat = (int32_t *)c->out_pat.p;
     // with page-locked results, each chunk of batches is copied back on the
-    // copy stream while the next chunks route
+    // copy stream while the next chunks route (inside the graph with GR_PLAN_GRAPH)
     auto pinned = [](const void *h) {
         cudaPointerAttributes a;
         if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
@@ -1155,29 +1213,15 @@ int gr_route_design_host(gr_ctx *c, int32_t n_nets, const int64_t *h_pin_ofs, co
         }
         return a.type == cudaMemoryTypeHost;
     };
-    const bool overlap = !(flags & GR_PLAN_GRAPH) && pinned(h_mst_edges) && (!h_mst_pat || pinned(h_mst_pat));
-    if (!overlap) {
-        rc = gr_route_plan(c, 0, n_batches, mst, pat, flags, nullptr);
+    if (pinned(h_mst_edges) && (!h_mst_pat || pinned(h_mst_pat))) {
+        rc = route_plan_impl(c, 0, n_batches, mst, pat, flags, c->stream, h_mst_edges, h_mst_pat);
+    } else {
+        rc = route_plan_impl(c, 0, n_batches, mst, pat, flags, c->stream, nullptr, nullptr);
         if (!rc) {
             GR_CK(cudaMemcpyAsync(h_mst_edges, mst, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream));
             if (h_mst_pat)
                 GR_CK(cudaMemcpyAsync(h_mst_pat, pat, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream));
         }
-    } else {
-        const int32_t chunk = 32;
-        for (int32_t b0 = 0; b0 < n_batches && !rc; b0 += chunk) {
-            const int32_t b1 = b0 + chunk < n_batches ? b0 + chunk : n_batches;
-            if ((rc = gr_route_plan(c, b0, b1, mst, pat, 0, nullptr))) break;
-            const int64_t s0 = c->plan[b0].slot0, s1 = b1 < n_batches ? c->plan[b1].slot0 : slots;
-            GR_CK(cudaEventRecord(c->ev_out, c->stream));
-            GR_CK(cudaStreamWaitEvent(c->copy_stream, c->ev_out, 0));
-            GR_CK(cudaMemcpyAsync(h_mst_edges + s0, mst + s0, sizeof(int64_t) * (s1 - s0), cudaMemcpyDeviceToHost,
-                                  c->copy_stream));
-            if (h_mst_pat)
-                GR_CK(cudaMemcpyAsync(h_mst_pat + s0, pat + s0, sizeof(int32_t) * (s1 - s0),
-                                      cudaMemcpyDeviceToHost, c->copy_stream));
-        }
-        GR_CK(cudaStreamSynchronize(c->copy_stream));
     }
     const int sr = gr_sync(c);
     return rc ? rc : sr;

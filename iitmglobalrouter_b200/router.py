@@ -221,11 +221,13 @@ class Router:
         check(self._lib.gr_route_plan(self._h, b0, b1, ptr(mst), ptr(mst_pat), GR_PLAN_GRAPH if graph else 0,
                                       stream), "gr_route_plan")
 
-    def route_design_host(self, pin_ofs, pins, batch_ofs, net_ids, mst_out, pat_out):
+    def route_design_host(self, pin_ofs, pins, batch_ofs, net_ids, mst_out, pat_out, graph=False):
+        """Upload, plan, route and copy back in one call (host arrays). graph:
+        the plan as a CUDA graph, reused while nothing it was built from changes."""
         pin_ofs, pins, batch_ofs, net_ids = i64(pin_ofs), i32(pins), i64(batch_ofs), i32(net_ids)
         check(self._lib.gr_route_design_host(self._h, len(pin_ofs) - 1, ptr(pin_ofs), ptr(pins),
                                              len(batch_ofs) - 1, ptr(batch_ofs), ptr(net_ids), ptr(mst_out),
-                                             ptr(pat_out), 0), "gr_route_design_host")
+                                             ptr(pat_out), GR_PLAN_GRAPH if graph else 0), "gr_route_design_host")
 
     def route_lookahead_host(self, net, every: int, beta: float, mode: str, mst_out, pat_out=None):
         """The uploaded plan routed from reset with the lookahead cost, all in

@@ -413,6 +413,38 @@ def test_route_design_host_end_to_end(cuda):
     assert np.array_equal(R.demand(), g.demand())
 
 
+def test_route_design_host_graph_reuse(cuda):
+    """The host-buffer entry in graph mode, called repeatedly on one context:
+    a graph is replayed while its plan's shapes and buffers are unchanged and
+    rebuilt when the design changes; every call gives the oracle's result,
+    with page-locked and with pageable output buffers."""
+    import torch
+
+    designs = [gr.Design.generate(1, seed=s) for s in (1, 2)]
+    X, Y, Z, cap, _, _ = design_arrays(designs[0])  # the second design's nets on the first one's grid
+    ref = []
+    for d in designs:
+        _, _, _, _, ofs, pins = design_arrays(d)
+        bofs, ids = d.batch(4)
+        g = oracle.Grid(X, Y, Z, cap)
+        rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=NT)
+        assert rc == 0
+        ref.append((ofs, pins, bofs, ids, mst_c, mp_c, g.demand()))
+    R = gr.Router(X, Y, Z, cap)
+    for k in (0, 0, 1, 0, 1, 1):
+        ofs, pins, bofs, ids, mst_c, mp_c, dem = ref[k]
+        for pinned in (True, False):
+            M = len(mst_c)
+            if pinned:
+                h_mst = torch.full((M,), -9, dtype=torch.int64).pin_memory().numpy()
+                h_pat = torch.full((M,), -9, dtype=torch.int32).pin_memory().numpy()
+            else:
+                h_mst, h_pat = np.full(M, -9, np.int64), np.full(M, -9, np.int32)
+            R.route_design_host(ofs, pins, bofs, ids, h_mst, h_pat, graph=True)
+            assert np.array_equal(h_mst, mst_c) and np.array_equal(h_pat, mp_c)
+            assert np.array_equal(R.demand(), dem)
+
+
 def test_contexts_of_different_sizes_coexist(cuda):
     """A context for a small grid created after one for a larger grid leaves
     the larger one routable (kernel attributes are process-wide)."""
