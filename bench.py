@@ -81,7 +81,8 @@ def learned_quality(d, R, mst, pat, n_batches, dims):
     """Quality of the design routed with the lookahead cost, when the package
     ships a network for this layer count (lookahead_z<Z>.npy with its
     lookahead_z<Z>.json report naming beta and the prediction interval);
-    the route's own time is reported beside it (not part of `value`)."""
+    the time of a second, warm learned route (identical to the first) is
+    reported beside it (not part of `value`)."""
     import torch
 
     from iitmglobalrouter_b200 import lookahead
@@ -94,10 +95,14 @@ def learned_quality(d, R, mst, pat, n_batches, dims):
     net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
                                  n_layers=rep["layers"])
     net.set_params(np.load(base.with_suffix(".npy")))
+    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta, mode=mode)  # warm-up
+    first = mst.cpu().numpy()
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta, mode=mode)
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
+    assert np.array_equal(mst.cpu().numpy(), first), "the learned route is not deterministic"
     out = lookahead.quality(d, R, mst, pat)
     out.update(beta=beta, every=every, mode=mode, route_ms=dt * 1e3, weights=base.with_suffix(".npy").name)
     R.reset()
