@@ -351,6 +351,13 @@ def main():
     kern_total = sum(v[0] for v in kern.values())
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / kern_total, 4)}
                for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}
+    # secondary figure: the bytes a direct Fenwick evaluation of every pattern
+    # would gather, over the time of the pattern stage (query tables + L-patterns)
+    gb = d.gather_bytes(threads=os.cpu_count() or 8)
+    pat_ms = sum(kernels[k]["ms"] for k in ("k_qtable", "k_lpat") if k in kernels)
+    gather = {"bytes_per_step": gb["bytes"], "valid_patterns": gb["patterns"], "pattern_stage_ms": pat_ms,
+              "gbs": gb["bytes"] / (pat_ms / 1e3) / 1e9 if pat_ms > 0 else None,
+              "note": "equivalent gather rate of the table-based pattern stage (no measured L2 peak to compare)"}
     # roofline of the dominant kernel: its algorithmic bytes per launch over
     # its average launch time in the profiled step; DRAM traffic per launch
     # from the ncu per-unit figures, scaled by the units one launch processes
@@ -421,6 +428,7 @@ def main():
                      "algorithmic_bytes_per_launch": alg_per_launch,
                      "step": {"achieved": step_achieved, "frac": step_achieved / peak, "algorithmic_bytes": bnet}},
         "kernels": kernels,
+        "gather": gather,
         "cpu_baseline": cpu,
         "e2e": {"value": replicas.whole_job_rate(n_nets, e2e_t, world), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},

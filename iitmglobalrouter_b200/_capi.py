@@ -83,6 +83,7 @@ SIGNATURES = {
     "gr_cnn_create": (_I, [_PP, _I, _I, _I, _I, _I, _I, _I, _U64]),
     "gr_cnn_destroy": (_I, [_P]),
     "gr_plan_check": (_I, [_P]),
+    "gr_design_gather_bytes": (_I, [_P, _I, _P]),
     "gr_cnn_num_params": (_I64, [_P]),
     "gr_cnn_info": (_I, [_P, _P, _P, _P, _P, _P]),
     "gr_route_design_lookahead_host": (_I, [_P, _P, C.c_int32, C.c_float, _I, _P, _P]),

@@ -1,4 +1,5 @@
 // gr_io_capi.cpp -- C ABI of the host-side design functions (gr_design_*).
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -135,6 +136,79 @@ int gr_design_write_routes(const gr_design *g, const char *path, const int64_t *
         wl_vias[1] = st.vias;
     }
     return rc;
+}
+
+int gr_design_gather_bytes(const gr_design *g, int threads, double *out2) {
+    if (!g || !out2) return GR_ERR_ARG;
+    const grio::Design &d = g->d;
+    const int Z = d.Z, Z2 = (Z + 1) / 2, np = Z * Z2;
+    if (Z < 2 || Z > 64) return GR_ERR_ARG;
+    // units (2 per wire segment + 1 per via cell) summed over the valid
+    // patterns of a pair, and the valid pattern count, by (z1, z2, kind):
+    // kind 0 stacked, 1 x differs only, 2 y differs only, 3 both differ
+    // (the validity and cell walk of the commit path's edge walk)
+    std::vector<int64_t> units((size_t)Z * Z * 4, 0), npat((size_t)Z * Z * 4, 0);
+    auto gap = [](int a, int b) { return a == b ? 0 : std::abs(a - b) - 1; };
+    for (int z1 = 0; z1 < Z; z1++)
+        for (int z2 = 0; z2 < Z; z2++)
+            for (int kind = 0; kind < 4; kind++) {
+                int64_t u = 0, n = 0;
+                for (int cp = 0; cp < np; cp++) {
+                    const int via1 = cp / Z2, v = cp % Z2, via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
+                    const bool bth = kind == 3;
+                    if (via1 < 1 || via1 >= Z || (bth && via2 != 0 && via2 >= Z)) continue;
+                    if (kind == 0) {  // the union of the layers between the pins and via1, via1 included
+                        uint64_t m = 1ull << via1;
+                        for (int i = std::min(z1, via1) + 1; i < std::max(z1, via1); i++) m |= 1ull << i;
+                        for (int i = std::min(via1, z2) + 1; i < std::max(via1, z2); i++) m |= 1ull << i;
+                        u += __builtin_popcountll(m);
+                        n++;
+                        continue;
+                    }
+                    // first wire on via1: even layers move x, odd ones y
+                    const bool moves_x = !(via1 & 1);
+                    bool xdone = kind == 2, ydone = kind == 1;
+                    if (moves_x) xdone = true;
+                    else ydone = true;
+                    int64_t cu = gap(z1, via1) + 2;
+                    int zl = via1;
+                    if (bth && via2 != 0 && via1 != via2) {
+                        cu += gap(via1, via2) + 2;
+                        if (!(via2 & 1)) xdone = true;
+                        else ydone = true;
+                        zl = via2;
+                    }
+                    if (!(xdone && ydone)) continue;  // does not reach the second pin
+                    if (kind == 1 && (via1 & 1)) continue;   // the wire moved y, which was already there
+                    if (kind == 2 && !(via1 & 1)) continue;  // the wire moved x
+                    cu += gap(zl, z2);
+                    u += cu;
+                    n++;
+                }
+                units[((size_t)z1 * Z + z2) * 4 + kind] = u;
+                npat[((size_t)z1 * Z + z2) * 4 + kind] = n;
+            }
+    double total = 0.0, pats = 0.0;
+    const int32_t nn = d.n_nets();
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : total, pats) num_threads(threads > 0 ? threads : 1)
+    for (int32_t i = 0; i < nn; i++) {
+        const int64_t o = d.pin_ofs[i], k = d.pin_ofs[i + 1] - o;
+        for (int64_t a = 0; a < k; a++) {
+            int za, xa, ya;
+            d.dec(d.pins[o + a], za, xa, ya);
+            for (int64_t b = a + 1; b < k; b++) {
+                int zb, xb, yb;
+                d.dec(d.pins[o + b], zb, xb, yb);
+                const int kind = (xa == xb && ya == yb) ? 0 : (ya == yb ? 1 : (xa == xb ? 2 : 3));
+                const size_t t = ((size_t)za * Z + zb) * 4 + kind;
+                total += (double)units[t];
+                pats += (double)npat[t];
+            }
+        }
+    }
+    out2[0] = 4.0 * total;
+    out2[1] = pats;
+    return GR_OK;
 }
 
 int gr_design_eval(const gr_design *g, const int32_t *demand, double *out3) {

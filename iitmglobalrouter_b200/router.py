@@ -112,6 +112,14 @@ class Design:
                                                threads, ptr(wv)), "gr_design_write_routes")
         return int(wv[0]), int(wv[1])
 
+    def gather_bytes(self, threads: int = 8) -> dict:
+        """Bytes a direct Fenwick evaluation of every pattern of every pin pair
+        would gather (4 B per unit: 2 per wire segment, 1 per via cell) and
+        the number of valid patterns."""
+        out = np.zeros(2, dtype=np.float64)
+        check(self._lib.gr_design_gather_bytes(self._h, threads, ptr(out)), "gr_design_gather_bytes")
+        return dict(bytes=float(out[0]), patterns=float(out[1]))
+
     def evaluate(self, demand) -> dict:
         demand = i32(demand)
         out = np.zeros(3, dtype=np.float64)

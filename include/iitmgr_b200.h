@@ -271,6 +271,11 @@ int gr_design_write_routes(const gr_design *d, const char *path, const int64_t *
                            int flags, int threads, int64_t *wl_vias);
 /* out3 = {overflow, overflowed cells, total demand} for a demand grid */
 int gr_design_eval(const gr_design *d, const int32_t *demand, double *out3);
+/* The secondary measurement figure (no counterpart in the reference): the
+ * bytes a direct Fenwick evaluation of every pattern of every pin pair
+ * would gather, 4 B x sum over pairs and valid patterns of (2 per wire
+ * segment + 1 per via cell), and the number of valid patterns: out2[0..1]. */
+int gr_design_gather_bytes(const gr_design *d, int threads, double *out2);
 
 /* ------------------------------------------------------------ congestion lookahead network
  * No counterpart in the reference: a stack of n_layers 3x3 convolutions

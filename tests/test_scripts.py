@@ -46,3 +46,68 @@ def test_bench_reference_arm_prints_one_json_line():
     assert out["impl"] == "reference" and out["unit"] == "nets/s" and out["value"] > 0
     assert out["cpu_baseline"]["kind"] == "port"
     assert out["e2e"]["h2d_bytes_per_step"] == 0 and out["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_gather_bytes_matches_a_literal_walk():
+    """The secondary measurement figure (bytes a direct Fenwick evaluation of
+    every pattern would gather) equals a pair-by-pair count that follows the
+    commit path's edge walk literally: a layer change costs one unit per
+    interior cell, a wire two, stacked pins the union of their layers."""
+    import numpy as np
+
+    import iitmglobalrouter_b200 as gr
+
+    d = gr.Design.generate(1, seed=3)
+    dims = d.dims
+    X, Y, Z = dims["X"], dims["Y"], dims["Z"]
+    Z2 = (Z + 1) // 2
+    ofs, pins = d.nets()
+
+    def dec(e):
+        z, r = divmod(int(e), X * Y)
+        return (z, r // Y, r % Y) if z & 1 else (z, r % X, r // X)
+
+    def walk(p, q, cp):
+        (z1, x1, y1), (z2, x2, y2) = p, q
+        via1, v = divmod(cp, Z2)
+        bth = x1 != x2 and y1 != y2
+        via2 = 2 * v if via1 & 1 else 2 * v + 1
+        if via1 < 1 or via1 >= Z or (bth and via2 != 0 and via2 >= Z):
+            return None
+        if (x1, y1) == (x2, y2):
+            cells = {via1} | set(range(min(z1, via1) + 1, max(z1, via1))) | set(range(min(via1, z2) + 1, max(via1, z2)))
+            return len(cells)
+        units = 0
+
+        def via(a, b):
+            return max(abs(a - b) - 1, 0)
+
+        units += via(z1, via1)
+        z = via1
+        units += 2
+        if z & 1:
+            y1 = y2
+        else:
+            x1 = x2
+        if bth and via2 != 0 and z != via2:
+            units += via(z, via2) + 2
+            z = via2
+            if z & 1:
+                y1 = y2
+            else:
+                x1 = x2
+        units += via(z, z2)
+        return units if (x1, y1) == (x2, y2) else None
+
+    total = pats = 0
+    for i in range(len(ofs) - 1):
+        p = [dec(e) for e in pins[ofs[i]:ofs[i + 1]]]
+        for a in range(len(p)):
+            for b in range(a + 1, len(p)):
+                for cp in range(Z * Z2):
+                    u = walk(p[a], p[b], cp)
+                    if u is not None:
+                        total += u
+                        pats += 1
+    got = d.gather_bytes(threads=4)
+    assert got["patterns"] == pats and got["bytes"] == 4 * total
