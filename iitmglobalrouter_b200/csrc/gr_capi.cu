@@ -40,6 +40,7 @@ struct BatchInfo {  // one batch of a plan
     int32_t max_pins;
     int32_t n2, nm, nl;  // nets of 2 pins, 3..32 pins, more
     int32_t nmid;        // of the nl larger nets, those up to kMstMidPins pins (listed first)
+    int64_t s2 = 0, sm = 0, smid = 0;  // MST slots of the 2-pin, 3..32-pin and mid classes
 };
 
 struct GraphCache {
@@ -107,6 +108,7 @@ struct gr_ctx {
     int32_t plan_max_pins = 0;  // largest net of the uploaded plan
     DevBuf plan_ids, plan_bofs, plan_pb;  // device plan builder: inputs, per-batch totals and an error flag
     DevBuf plan_slot0, slot_net;          // per batch its first MST slot; per plan slot its net
+    DevBuf slot_ord;                      // per batch its slots in class order (k_plan_slot_order)
     bool h_nxy_valid = false;             // h_nxy mirrors d_nxy (copied when a host-built descriptor needs it)
     int *d_queue = nullptr;  // k_mst_queue: next item, CTAs finished (zero between launches)
     int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
@@ -269,6 +271,14 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
     bi.nm = nm;
     bi.nl = n - n2 - nm;
     bi.nmid = nmid;
+    bi.s2 = 2 * (int64_t)n2;
+    bi.sm = 0;
+    bi.smid = 0;
+    for (int32_t i = 0; i < n; i++) {
+        const int32_t k = npin[i];
+        if (k != 2 && k <= kMstWarpPins) bi.sm += k;
+        else if (k > kMstWarpPins && k <= kMstMidPins) bi.smid += k;
+    }
     bi.first = first;
     bi.n = n;
     bi.n_pairs = P;
@@ -288,6 +298,9 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
     v.nm = bi.nm;
     v.nl = bi.nl;
     v.nmid = bi.nmid;
+    v.s2 = bi.s2;
+    v.sm = bi.sm;
+    v.smid = bi.smid;
     return v;
 }
 
@@ -362,8 +375,33 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
     return GR_OK;
 }
 
+// What the marking needs besides the batch view: the pair patterns and where
+// the slots' patterns go.
+struct MarkArgs {
+    const int16_t *ppat;
+    int32_t *mst_pat;
+};
+
+// k_mark7 over slots k0..k1-1 (entries of v.slot_ord when set) on stream s
+int launch_mark(gr_ctx *c, const BatchView &v, const int64_t *mst, const MarkArgs &mk, int64_t k0, int64_t k1,
+                cudaStream_t s) {
+    if (k1 <= k0) return GR_OK;
+    int pi = prof_begin(c, s);
+    k_mark7<<<grid_for(c, (k1 - k0) * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, mk.ppat, mk.mst_pat, c->d_mark,
+                                                               c->d_tbits, c->d_tlist, c->d_list_count, c->d_status,
+                                                               v.slot_ord, k0, k1);
+    prof_end(c, s, pi, GR_K_MARK);
+    GR_CK(cudaGetLastError());
+    return GR_OK;
+}
+
+// mk (plans only, v.slot_ord set, the track count already cleared and the
+// 2-pin trees already written): each size class's slots are marked on the
+// class's stream right after its trees, so the marking of the small classes
+// overlaps the Boruvka of the large nets and only the largest class's marking
+// remains on the batch's critical path
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s,
-               bool pin2_done = false) {
+               bool pin2_done = false, const MarkArgs *mk = nullptr) {
     if (v.n <= 0) return GR_OK;
     if (c->tune[GR_TUNE_MST_QUEUE]) {
         if (v.n2 > 0 && !pin2_done) {
@@ -414,6 +452,10 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s0>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s0, pi, GR_K_MST_WARP);
     }
+    if (mk && v.s2 + v.sm > 0) {
+        int rc = launch_mark(c, v, mst, *mk, 0, v.s2 + v.sm, side(0));
+        if (rc) return rc;
+    }
     // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above. A
     // net's full cost matrix sits in the CTA's shared memory when it fits, is
     // spread over a 4- or 8-CTA cluster when that fits, else goes to a per-CTA
@@ -463,6 +505,11 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
                                                               (int64_t)maxn * maxn, first, cnt);
         }
         prof_end(c, sp, pi, GR_K_MST_LARGE);
+        if (mk) {
+            const int64_t k0 = v.s2 + v.sm + (part ? v.smid : 0);
+            int rc = launch_mark(c, v, mst, *mk, k0, part ? v.n_nodes : k0 + v.smid, sp);
+            if (rc) return rc;
+        }
     }
     for (int i = 0; i < 3; i++)
         if (used[i]) {
@@ -479,16 +526,18 @@ constexpr int kTrackCapMax = 1024;   // marked cells per track kept in shared me
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
 
 // count_cleared: an L-pattern kernel of this batch already set the track count to 0
+// marked: launch_mst already marked the batch's slots
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
-                  cudaStream_t s, bool count_cleared = false) {
+                  cudaStream_t s, bool count_cleared = false, bool marked = false) {
     if (v.n_nodes <= 0) return GR_OK;
-    if (!count_cleared) GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
+    if (!marked) {
+        if (!count_cleared) GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
+        BatchView va = v;
+        va.slot_ord = nullptr;  // all slots in batch order
+        int rc = launch_mark(c, va, mst, MarkArgs{ppat, mst_pat}, 0, v.n_nodes, s);
+        if (rc) return rc;
+    }
     int pi = prof_begin(c, s);
-    k_mark7<<<grid_for(c, v.n_nodes * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, ppat, mst_pat, c->d_mark,
-                                                                c->d_tbits, c->d_tlist, c->d_list_count,
-                                                                c->d_status);
-    prof_end(c, s, pi, GR_K_MARK);
-    pi = prof_begin(c, s);
     int64_t blocks = ((int64_t)c->n_tracks + kTrackWarps - 1) / kTrackWarps;
     if (blocks > (int64_t)c->sm_count * 8) blocks = (int64_t)c->sm_count * 8;
     k_track_commit<<<(int)blocks, kTrackWarps * 32, track_smem(c->track_cap), s>>>(
@@ -574,8 +623,12 @@ int route_one(gr_ctx *c, const BatchView &v, int64_t *mst, int32_t *mst_pat, flo
     BatchView vl = v;  // the L-pattern kernel also clears the marking's track count
     vl.zero_count = c->d_list_count;
     if ((rc = launch_lpat_batch(c, vl, pcost, ppat, (float2 *)c->tab.p, s, mst, dist))) return rc;
-    if ((rc = launch_mst(c, v, pcost, mst, dist, s, true))) return rc;
-    return launch_commit(c, v, mst, ppat, mst_pat, s, v.n_pairs > 0);
+    // per-class marking on the Boruvka streams needs the class-ordered slot
+    // list of a plan and the track count cleared by the L-pattern kernel
+    const bool split = v.slot_ord && v.n_pairs > 0 && !c->tune[GR_TUNE_MST_QUEUE];
+    const MarkArgs mk{ppat, mst_pat};
+    if ((rc = launch_mst(c, v, pcost, mst, dist, s, true, split ? &mk : nullptr))) return rc;
+    return launch_commit(c, v, mst, ppat, mst_pat, s, v.n_pairs > 0, split);
 }
 
 void free_buf(DevBuf &b) {
@@ -780,6 +833,7 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->plan_pb);
     free_buf(c->plan_slot0);
     free_buf(c->slot_net);
+    free_buf(c->slot_ord);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -1012,6 +1066,9 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
         bi.nm = q.nm;
         bi.nmid = q.nmid;
         bi.nl = bi.n - q.n2 - q.nm;
+        bi.s2 = q.s2;
+        bi.sm = q.sm;
+        bi.smid = q.smid;
         if ((rc = check_mst_smem(c, bi.max_pins))) return rc;
     }
     for (int32_t b = 0; b < n_batches; b++) {
@@ -1037,6 +1094,12 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
                               c->stream));
         k_plan_slots<<<n_batches, 256, 0, c->stream>>>((const int64_t *)c->plan_bofs.p, (const int64_t *)c->plan_slot0.p,
                                                       all.npin, all.node_ofs, (int32_t *)c->slot_net.p);
+        c->launches++;
+        // slots in class order: each size class is marked on its own stream
+        if ((rc = ensure(c->slot_ord, sizeof(int32_t) * (size_t)slot, c->stream))) return rc;
+        k_plan_slot_order<<<n_batches, 1024, 0, c->stream>>>((const int64_t *)c->plan_bofs.p,
+                                                            (const int64_t *)c->plan_slot0.p, all.npin, all.node_ofs,
+                                                            all.order, (int32_t *)c->slot_ord.p);
         c->launches++;
         GR_CK(cudaGetLastError());
     }
@@ -1070,9 +1133,23 @@ int gr_plan_check(gr_ctx *c) {
         BatchInfo hb{};
         if ((rc = fill_desc(c, ids.data() + bi.first, bi.n, host.data(), total, bi.first, hb))) return rc;
         bad |= hb.n_pairs != bi.n_pairs || hb.n_nodes != bi.n_nodes || hb.n_tab != bi.n_tab ||
-               hb.max_pins != bi.max_pins || hb.n2 != bi.n2 || hb.nm != bi.nm || hb.nl != bi.nl || hb.nmid != bi.nmid;
+               hb.max_pins != bi.max_pins || hb.n2 != bi.n2 || hb.nm != bi.nm || hb.nl != bi.nl || hb.nmid != bi.nmid ||
+               hb.s2 != bi.s2 || hb.sm != bi.sm || hb.smid != bi.smid;
     }
     bad |= memcmp(dev.data(), host.data(), bytes - 64) != 0;
+    // the class-ordered slot list against the host descriptor's order
+    if (!bad && c->plan_slots > 0 && c->slot_ord.p) {
+        std::vector<int32_t> so((size_t)c->plan_slots);
+        GR_CK(cudaMemcpy(so.data(), c->slot_ord.p, sizeof(int32_t) * so.size(), cudaMemcpyDeviceToHost));
+        for (const BatchInfo &bi : c->plan) {
+            const BatchView hv = view_of(host.data(), total, bi.first, bi.n);
+            int64_t k = bi.slot0;
+            for (int32_t p = 0; p < bi.n && !bad; p++) {
+                const int32_t i = hv.order[p];
+                for (int32_t j = 0; j < hv.npin[i]; j++) bad |= so[(size_t)k++] != (int32_t)hv.node_ofs[i] + j;
+            }
+        }
+    }
     return bad ? GR_ERR_DEVICE : GR_OK;
 }
 
@@ -1088,7 +1165,7 @@ std::vector<uint64_t> graph_sig(const gr_ctx *c, int32_t b0, int32_t b1, const v
                                 cudaStream_t s, const void *h_mst, const void *h_pat) {
     std::vector<uint64_t> v;
     auto P = [&](const void *p) { v.push_back((uint64_t)(uintptr_t)p); };
-    const void *const ptrs[] = {mst, pat, (const void *)s, h_mst, h_pat, c->plan_desc.p, c->slot_net.p, c->pcost.p,
+    const void *const ptrs[] = {mst, pat, (const void *)s, h_mst, h_pat, c->plan_desc.p, c->slot_net.p, c->slot_ord.p, c->pcost.p,
                           c->ppat.p, c->tab.p, c->dist.p, c->mat.p, (const void *)c->d_pins, (const void *)c->d_pxy,
                           (const void *)c->d_cx, (const void *)c->d_cy, (const void *)c->d_fen, (const void *)c->d_capr,
                           (const void *)c->d_mark, (const void *)c->d_tbits, (const void *)c->d_tlist,
@@ -1105,7 +1182,7 @@ std::vector<uint64_t> graph_sig(const gr_ctx *c, int32_t b0, int32_t b1, const v
     for (int32_t b = b0; b < b1; b++) {
         const BatchInfo &bi = c->plan[b];
         const int64_t f[] = {bi.first, (int64_t)bi.n, bi.n_pairs, bi.n_nodes, bi.n_tab, bi.slot0, (int64_t)bi.max_pins,
-                             (int64_t)bi.n2, (int64_t)bi.nm, (int64_t)bi.nl, (int64_t)bi.nmid};
+                             (int64_t)bi.n2, (int64_t)bi.nm, (int64_t)bi.nl, (int64_t)bi.nmid, bi.s2, bi.sm, bi.smid};
         for (int64_t x : f) v.push_back((uint64_t)x);
     }
     return v;
@@ -1126,6 +1203,7 @@ int route_plan_impl(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int
             const BatchInfo &bi = c->plan[b];
             BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
             if (c->slot_net.p) v.slot_net = (const int32_t *)c->slot_net.p + bi.slot0;
+            if (c->slot_ord.p) v.slot_ord = (const int32_t *)c->slot_ord.p + bi.slot0;
             int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr,
                                (float *)c->dist.p, (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
             if (rc) return rc;

@@ -41,6 +41,8 @@ struct BatchView {
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
     int32_t nmid;             // of the nl larger nets, the first nmid have at most 128 pins
     const int32_t *slot_net;  // [n_nodes] net of each MST slot (plans only; null: found by search)
+    const int32_t *slot_ord;  // [n_nodes] the batch's slots, nets in `order` (plans only, else null)
+    int64_t s2, sm, smid;     // MST slots of the 2-pin, 3..32-pin and 33..128-pin classes (plans only)
     int32_t *zero_count;      // set to 0 by the L-pattern kernel (the marking's track count), or null
 };
 
@@ -301,6 +303,7 @@ __global__ void __launch_bounds__(128) k_fen_tracks(GridC g, int n_tracks, int l
 // batch.
 struct PlanBatch {  // per-batch totals for the host's launch shapes
     int64_t n_pairs, n_nodes, n_tab;
+    int64_t s2, sm, smid;  // MST slots of the 2-pin, 3..warp_pins and ..mid_pins classes
     int32_t max_pins, n2, nm, nmid;
 };
 
@@ -372,6 +375,7 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
     __syncthreads();
     // pass 1: offsets, class counts, largest net
     int64_t P = 0, Mn = 0, T = 0;
+    int64_t k0 = 0, k1 = 0, k2 = 0;  // this thread's MST slots per class
     int c0 = 0, c1 = 0, c2 = 0;
     for (int base = 0; base < n; base += blockDim.x) {
         const int i = base + tid;
@@ -396,10 +400,15 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
         Mn += tb;
         T += tc;
         const int q = i < n ? cls(k) : -1;
+        k0 += q == 0 ? k : 0;
+        k1 += q == 1 ? k : 0;
+        k2 += q == 2 ? k : 0;
         c0 += __syncthreads_count(q == 0);
         c1 += __syncthreads_count(q == 1);
         c2 += __syncthreads_count(q == 2);
     }
+    int64_t S0, S1, S2;
+    block_excl_scan3(k0, k1, k2, S0, S1, S2, wsum);
     // pass 2: stable partition by class
     int run[4] = {0, c0, c0 + c1, c0 + c1 + c2};
     for (int base = 0; base < n; base += blockDim.x) {
@@ -430,11 +439,48 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
         pb.n_pairs = P;
         pb.n_nodes = Mn;
         pb.n_tab = T;
+        pb.s2 = S0;
+        pb.sm = S1;
+        pb.smid = S2;
         pb.max_pins = s_max;
         pb.n2 = c0;
         pb.nm = c1;
         pb.nmid = c2;
         out[blockIdx.x] = pb;
+    }
+}
+
+// The plan's class-ordered slot list: batch b's slots, net by net in the
+// batch's `order` (2-pin nets, then 3..32 pins, 33..128, larger), each net's
+// slots in turn; entries are slot indices relative to the batch. The marking
+// of one size class then covers a contiguous range of the list. One CTA
+// (1024 threads) per batch.
+__global__ void __launch_bounds__(1024) k_plan_slot_order(const int64_t *__restrict__ bofs,
+                                                          const int64_t *__restrict__ slot0,
+                                                          const int32_t *__restrict__ npin,
+                                                          const int64_t *__restrict__ node_ofs,
+                                                          const int32_t *__restrict__ order,
+                                                          int32_t *__restrict__ slot_ord) {
+    __shared__ int64_t wsum[32][3];
+    const int64_t first = bofs[blockIdx.x];
+    const int n = (int)(bofs[blockIdx.x + 1] - first);
+    int32_t *dst = slot_ord + slot0[blockIdx.x];
+    int64_t run = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int p = base + threadIdx.x;
+        int i = 0;
+        int64_t k = 0, z1 = 0, z2 = 0, t0, t1, t2;
+        if (p < n) {
+            i = order[first + p];
+            k = npin[first + i];
+        }
+        block_excl_scan3(k, z1, z2, t0, t1, t2, wsum);  // k: this net's first position in the list
+        if (p < n) {
+            const int32_t s = (int32_t)node_ofs[first + i];
+            const int cnt = npin[first + i];
+            for (int j = 0; j < cnt; j++) dst[run + k + j] = s + j;
+        }
+        run += t0;
     }
 }
 
@@ -1383,21 +1429,28 @@ __device__ __forceinline__ void track_of(const GridC &g, int32_t e, int &t, int3
     base = z * g.XY + row * L;
 }
 
-// One warp per MST slot, as k_mark6, but what the batch records is the set
-// of tracks that gained marked cells: each path unit (a via cell, or the
-// part of a wire inside one 32-cell mark word) lies in a single track, and
-// the first unit to set bits of a track flags it in a track bitmap and
-// appends the track's first cell to the track list.
+// One warp per MST slot (mst_bit_commit.hpp:147-235): the warp walks the
+// slot's L path and sets the mark bits of its GCELLs with atomicOr. What the
+// batch records is the set of tracks that gained marked cells: each path
+// unit (a via cell, or the part of a wire inside one 32-cell mark word) lies
+// in a single track, and the first unit to set bits of a track flags it in a
+// track bitmap and appends the track's first cell to the track list.
+// Slots k0..k1-1 of the batch are marked; with `sorder` they are entries
+// k0..k1-1 of the class-ordered slot list, so that each size class can be
+// marked on its own stream right after its trees are built (marking is
+// order-independent: bits are ORed, tracks listed as a set).
 __global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
                                                int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *tbits,
-                                               int32_t *__restrict__ tlist, int32_t *tcount, uint32_t *status) {
+                                               int32_t *__restrict__ tlist, int32_t *tcount, uint32_t *status,
+                                               const int32_t *__restrict__ sorder, int64_t k0, int64_t k1) {
     __shared__ PathUnits su[8];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     PathUnits &pu = su[wib];
-    for (int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; s < bv.n_nodes; s += nwarps) {
+    for (int64_t kk = k0 + (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; kk < k1; kk += nwarps) {
+        const int64_t s = sorder ? (int64_t)__ldg(sorder + kk) : kk;
         int units = 0;
         const int net = bv.slot_net ? __ldg(bv.slot_net + s) : warp_ofs_search(bv.node_ofs, bv.n, s, lane);
         if (lane == 0) {
