@@ -1557,28 +1557,49 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
             if (m) {
                 uint32_t b = m;
                 while (b) {
-                    const int e = (w << 5) + __ffs(b) - 1;
+                    P[k++] = (w << 5) + __ffs(b) - 1 - base;
                     b &= b - 1;
-                    const int cv = capr[e];
-                    P[k] = e - base;
-                    if (pred) {
-                        const float pe = __ldg(pred + e);
-                        D[k] = la_cost(cv - 1, pe, beta) - la_cost(cv, pe, beta);
-                    } else {
-                        D[k] = __ldg(dlut + (cv < kLutMin ? 0 : (cv > kLutMax + 1 ? kLutMax + 1 - kLutMin : cv - kLutMin)));
-                    }
-                    capr[e] = cv - 1;
-                    k++;
                 }
                 atomicAnd(mark + w, ~m);
             }
         }
         __syncwarp();
-        // (2) node updates, one owner per node
-        for (int k = lane; k < total; k += 32) {
+        // capacities and increments, lane-parallel with four gathers in flight
+        for (int k0 = lane; k0 < total; k0 += 128) {
+            int cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + 32 * u;
+                cv[u] = k < total ? capr[base + P[k]] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int k = k0 + 32 * u;
+                if (k < total) {
+                    const int e = base + P[k];
+                    if (pred) {
+                        const float pe = __ldg(pred + e);
+                        D[k] = la_cost(cv[u] - 1, pe, beta) - la_cost(cv[u], pe, beta);
+                    } else {
+                        const int c = cv[u];
+                        D[k] = __ldg(dlut + (c < kLutMin ? 0 : (c > kLutMax + 1 ? kLutMax + 1 - kLutMin : c - kLutMin)));
+                    }
+                    capr[e] = cv[u] - 1;
+                }
+            }
+        }
+        __syncwarp();
+        // (2) node updates, one owner per node. Row r of 32 compacted cells
+        // goes to the lanes rotated by r: on a densely marked track the owners
+        // of the large nodes (cells 32r+31) then fall on different lanes
+        // instead of all on lane 31.
+        for (int r = 0; 32 * r < total; r++) {
+            const int k = 32 * r + ((lane + r) & 31);
+            if (k >= total) continue;
             const int p = P[k];
             const int nxt = k + 1 < total ? P[k + 1] : L;  // next marked position (L: none)
             for (int i = p + 1; i <= L && nxt >= i; i += i & -i) {
+                float v = fen[base + i - 1];  // in flight during the search
                 const int lo = i - (i & -i);  // range [lo, i-1], 0-based
                 int a = 0, b = k;             // first index with P >= lo
                 while (a < b) {
@@ -1586,8 +1607,17 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
                     if (P[mid] < lo) a = mid + 1;
                     else b = mid;
                 }
-                float v = fen[base + i - 1];
-                for (int j = a; j <= k; j++) v += D[j];
+                // the range's increments in cell order, eight loads ahead of
+                // their additions
+                int j = a;
+                for (; j + 8 <= k + 1; j += 8) {
+                    float d[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) d[u] = D[j + u];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) v += d[u];
+                }
+                for (; j <= k; j++) v += D[j];
                 fen[base + i - 1] = v;
             }
         }
