@@ -1204,8 +1204,9 @@ int route_plan_impl(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int
             BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
             if (c->slot_net.p) v.slot_net = (const int32_t *)c->slot_net.p + bi.slot0;
             if (c->slot_ord.p) v.slot_ord = (const int32_t *)c->slot_ord.p + bi.slot0;
-            int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr,
-                               (float *)c->dist.p, (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
+            // no per-net tree costs: a plan returns trees and patterns only
+            int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr, nullptr,
+                               (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
             if (rc) return rc;
             if (h_mst && ((b + 1 - b0) % chunk == 0 || b + 1 == b1)) {
                 const int32_t c0 = b + 1 - ((b + 1 - b0) % chunk ? (b + 1 - b0) % chunk : chunk);

@@ -698,9 +698,11 @@ __device__ __forceinline__ void mst_scan_row(const MstArrays &a, const uint32_t 
 // is not null), sum their costs into d in that order, and merge. A merged
 // component's root is its largest pin index (union points the smaller root
 // at the larger one), found by following each candidate's chain to its
-// tree's top. Returns the number of edges recorded this round.
+// tree's top. Returns the number of edges recorded this round. want_d false
+// (the caller keeps no per-net sums) skips the sum, a serial step of one
+// thread per round.
 __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net, int nrec, int64_t *out, float &d,
-                                              int *warp_sums, int *s_total, uint32_t *status) {
+                                              int *warp_sums, int *s_total, uint32_t *status, bool want_d) {
     const int B = blockDim.x, tid = threadIdx.x;
     for (int v = tid; v < n; v += B) {
         int s = -1;
@@ -734,10 +736,11 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
     for (int v = c0; v < c1; v++)
         if (a.flag[v]) {
             if (out) out[nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)a.sel[v];
-            a.wrec[pos++] = key_cost(a.key[v]);
+            if (want_d) a.wrec[pos] = key_cost(a.key[v]);
+            pos++;
         }
     __syncthreads();
-    if (tid == 0) {
+    if (want_d && tid == 0) {
         float dd = d;
         for (int i = 0; i < total; i++) dd += a.wrec[i];
         d = dd;
@@ -809,7 +812,7 @@ __device__ __forceinline__ void mst_block_net(const BatchView &bv, const float *
         __syncthreads();
         for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * n, v, n, lane);
         __syncthreads();
-        nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, s_total, status);
+        nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, s_total, status, dist != nullptr);
     }
     for (int v = nrec + tid; v < n; v += B) out[v] = -1;
     if (tid == 0) {
@@ -894,7 +897,7 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
             }
             cl.sync();  // remote reads done before the partials are reset
             nrec += mst_round_tail(a, n, net, nrec, rank == 0 ? mst + bv.node_ofs[net] : nullptr, d, warp_sums,
-                                   &s_total, status);
+                                   &s_total, status, dist != nullptr);
         }
         if (rank == 0) {
             int64_t *out = mst + bv.node_ofs[net];
@@ -1198,10 +1201,12 @@ __device__ __forceinline__ void mst_warp_net(const BatchView &bv, const float *_
         const unsigned recm = __ballot_sync(FULL, rec);
         if (rec)
             out[nrec + __popc(recm & ((1u << lane) - 1))] = ((int64_t)i << 30) | ((int64_t)lane << 15) | (int64_t)sel;
-        const float wv = rec ? w[(uint32_t)mykey] : 0.0f;
-        for (int v = 0; v < 32; v++) {
-            const float x = __shfl_sync(FULL, wv, v);
-            if ((recm >> v) & 1u) d += x;
+        if (dist) {  // the round's costs in lane order (uniform branch)
+            const float wv = rec ? w[(uint32_t)mykey] : 0.0f;
+            for (int v = 0; v < 32; v++) {
+                const float x = __shfl_sync(FULL, wv, v);
+                if ((recm >> v) & 1u) d += x;
+            }
         }
         nrec += __popc(recm);
         // tops of the candidate trees, then each tree's largest root
