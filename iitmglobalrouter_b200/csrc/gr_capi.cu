@@ -521,6 +521,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
 }
 
 constexpr int kTrackWarps = 8;       // warps per k_track_commit block
+static_assert(kTrackWarps <= kTrackWarpsMax, "k_track_commit's per-warp rank tables");
 constexpr int kTrackCapMax = 1024;   // marked cells per track kept in shared memory
 
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }

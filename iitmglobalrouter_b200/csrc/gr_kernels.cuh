@@ -1502,6 +1502,10 @@ __global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int3
     }
 }
 
+constexpr int kTrackWarpsMax = 8;  // warps per k_track_commit block
+constexpr int kTrackWords = 48;    // mark words per track in the node sweep's rank table
+constexpr int kTrackSweepMin = 64; // tracks with more marked cells update by node
+
 // One warp per listed track (bit_util.hpp:75-90 for the cells the batch
 // marked on it): (1) the marked positions of the track and their increments
 // cost(cap-1) - cost(cap) are compacted in ascending order (shared memory
@@ -1519,8 +1523,13 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
                                                       int32_t *__restrict__ gpos, float *__restrict__ gdel,
                                                       int cap, const float *__restrict__ pred, float beta) {
     extern __shared__ int32_t tsm[];  // per warp: cap positions, then cap increments
+    // per warp: the track's mark words and the marked cells before each word
+    __shared__ uint32_t s_wm[kTrackWarpsMax][kTrackWords];
+    __shared__ int s_wk[kTrackWarpsMax][kTrackWords];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    uint32_t *wm = s_wm[wib];
+    int *wk = s_wk[wib];
     const int cnt = *tcount;
     int32_t *spos = tsm + (size_t)wib * 2 * cap;
     float *sdel = reinterpret_cast<float *>(spos + cap);
@@ -1540,6 +1549,10 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
         total = __reduce_add_sync(FULL, total);
         int32_t *P = total <= cap ? spos : gpos + base;
         float *D = total <= cap ? sdel : gdel + base;
+        // heavily marked tracks update by node (the per-cell walks would
+        // chain many dependent node loads on a few lanes); the words must fit
+        // the rank table
+        const bool sweep = total > kTrackSweepMin && w1 - w0 + 2 <= kTrackWords;
         // (1) compaction in position order
         int run = 0;
         for (int c0 = w0; c0 <= w1; c0 += 32) {
@@ -1559,6 +1572,10 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
             }
             int k = run + incl - pc;
             run += __shfl_sync(FULL, incl, 31);
+            if (sweep && w <= w1) {
+                wm[w - w0] = m;
+                wk[w - w0] = k;
+            }
             if (m) {
                 uint32_t b = m;
                 while (b) {
@@ -1567,6 +1584,10 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
                 }
                 atomicAnd(mark + w, ~m);
             }
+        }
+        if (sweep && lane == 0) {  // one word past the track: rank(L) = total
+            wm[w1 - w0 + 1] = 0;
+            wk[w1 - w0 + 1] = total;
         }
         __syncwarp();
         // capacities and increments, lane-parallel with four gathers in flight
@@ -1594,6 +1615,59 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
             }
         }
         __syncwarp();
+        if (sweep) {
+            // (2) node updates by node: every node whose range (i - lowbit(i),
+            // i] holds marked cells gets those cells' increments added in
+            // cell order (the same sum as below). Lanes take the nodes in
+            // rows of 32, rotated by the row so that the large nodes (i a
+            // multiple of 32) spread over the warp; a node's marked cells are
+            // compacted entries rank(lo) .. rank(i) - 1, read from the word
+            // table; eight nodes' loads are in flight per lane.
+            const int off = base & 31;
+            auto rank = [&](int q) {  // marked cells of the track before position q
+                const int e = q + off;
+                return wk[e >> 5] + __popc(wm[e >> 5] & ((1u << (e & 31)) - 1u));
+            };
+            const int rows = (L + 31) >> 5;
+            for (int r0 = 0; r0 < rows; r0 += 8) {
+                float v[8];
+                int a8[8], b8[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int r = r0 + u;
+                    const int i = 32 * r + ((lane + r) & 31) + 1;
+                    a8[u] = 0;
+                    b8[u] = -1;
+                    v[u] = 0.0f;
+                    if (r < rows && i <= L) {
+                        const int ra = rank(i - (i & -i)), rb = rank(i);
+                        if (rb > ra) {
+                            a8[u] = ra;
+                            b8[u] = rb - 1;
+                            v[u] = fen[base + i - 1];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (b8[u] < a8[u]) continue;
+                    const int r = r0 + u;
+                    const int i = 32 * r + ((lane + r) & 31) + 1;
+                    float x = v[u];
+                    int j = a8[u];
+                    const int k = b8[u];
+                    for (; j + 8 <= k + 1; j += 8) {
+                        float d[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) d[t] = D[j + t];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) x += d[t];
+                    }
+                    for (; j <= k; j++) x += D[j];
+                    fen[base + i - 1] = x;
+                }
+            }
+        } else
         // (2) node updates, one owner per node. Row r of 32 compacted cells
         // goes to the lanes rotated by r: on a densely marked track the owners
         // of the large nodes (cells 32r+31) then fall on different lanes

@@ -368,6 +368,37 @@ def test_edge_cases_small_grids(cuda):
         R.sync()
 
 
+@pytest.mark.parametrize("X", [300, 1000])
+def test_dense_tracks_bitexact(cuda, X):
+    """Batches that mark hundreds of cells of one track (rows of disjoint
+    2-pin nets along x): the commit updates such tracks node by node. Track
+    lengths 300 and 1000 start at cells that are not multiples of 32."""
+    Y, Z = 7, 3
+    cap = (np.arange(X * Y * Z, dtype=np.int32) % 7 + 3).astype(np.int32)
+    g = oracle.Grid(X, Y, Z, cap)
+    nets = []
+    for shift in (0, 4):  # the second batch overlaps the first one's wires
+        for y in range(Y):
+            for x0 in range(shift, X - 9, 10):
+                nets.append(sorted({g.enc(0, x0, y), g.enc(0, x0 + 8, y), g.enc(y % 2, x0 + 3, y)}))
+    ofs = np.cumsum([0] + [len(q) for q in nets]).astype(np.int64)
+    pins = np.concatenate([np.array(q, np.int32) for q in nets])
+    half = len(nets) // 2
+    bofs = np.array([0, half, len(nets)], np.int64)
+    ids = np.arange(len(nets), dtype=np.int32)
+    rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=NT)
+    assert rc == 0
+    R = gr.Router(X, Y, Z, cap)
+    R.set_nets(ofs, pins)
+    mst, mp = route_all_gpu(R, ofs, bofs, ids, "plan")
+    assert np.array_equal(mst, mst_c) and np.array_equal(mp, mp_c)
+    assert np.array_equal(R.capr(), g.capr())
+    assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))
+    # some track of layer 2 gained more than 64 units of demand in one batch
+    dem = (cap - R.capr()).reshape(Z, Y, X)
+    assert int((dem[2] > 0).sum(axis=1).max()) > 64
+
+
 def test_invalid_inputs_reported_not_faulted(cuda):
     import torch
 
