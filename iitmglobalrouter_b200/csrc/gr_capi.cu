@@ -522,7 +522,10 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
 
 constexpr int kTrackWarps = 8;       // warps per k_track_commit block
 static_assert(kTrackWarps <= kTrackWarpsMax, "k_track_commit's per-warp rank tables");
-constexpr int kTrackCapMax = 1024;   // marked cells per track kept in shared memory
+// marked cells per track kept in shared memory (more go to the track's slice
+// of the global scratch): 16 KB per 8-warp block, so eight blocks fit an SM
+// and a batch's touched tracks (up to ~10K) run in one wave
+constexpr int kTrackCapMax = 256;
 
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
 
