@@ -1020,7 +1020,7 @@ __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, 
 }
 
 template <int ZC>
-__global__ void __launch_bounds__(256, 2) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
+__global__ void __launch_bounds__(256, 3) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
                                                 float *__restrict__ cost, int16_t *__restrict__ pat,
                                                 int64_t *__restrict__ mst, float *__restrict__ dist) {
