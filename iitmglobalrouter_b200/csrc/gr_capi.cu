@@ -452,8 +452,9 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s0>>>(c->g, v, pcost, mst, dist, c->d_status);
         prof_end(c, s0, pi, GR_K_MST_WARP);
     }
-    if (mk && v.s2 + v.sm > 0) {
-        int rc = launch_mark(c, v, mst, *mk, 0, v.s2 + v.sm, side(0));
+    if (mk) {  // 2-pin trees exist since the L-pattern kernel: marked beside every class's Boruvka
+        int rc = launch_mark(c, v, mst, *mk, 0, v.s2, s);
+        if (!rc && v.sm > 0) rc = launch_mark(c, v, mst, *mk, v.s2, v.s2 + v.sm, side(0));
         if (rc) return rc;
     }
     // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above. A
