@@ -201,16 +201,45 @@ def cpu_sample(ofs, pins, bofs, ids, target_pairs):
     return np.array(sofs, np.int64), np.concatenate(sids).astype(np.int32), stride, len(sel)
 
 
-def time_oracle(d, ofs, pins, sofs, sids, nthreads):
+def time_oracle(d, ofs, pins, sofs, sids, nthreads, keep=False):
+    """The oracle routes the sample's batches in order from the initial cost
+    state (its Fenwick build inside the timed region, as the GPU step's
+    reset is); with keep, also returns its grid and results."""
     import oracle
 
     dims = d.dims
     g = oracle.Grid(dims["X"], dims["Y"], dims["Z"], d.caps())
     t0 = time.perf_counter()
-    rc, _, _ = g.route_batches(ofs, pins, sofs, sids, nthreads=nthreads)
+    g.reset()
+    rc, mst, pat = g.route_batches(ofs, pins, sofs, sids, nthreads=nthreads)
     dt = time.perf_counter() - t0
     assert rc == 0
+    if keep:
+        return len(sids) / dt, dt, (g, mst, pat)
     return len(sids) / dt, dt
+
+
+def sample_parity(R, sofs, sids, ref):
+    """The GPU routes the oracle's sample (the same batches, in the same
+    order, from the same initial state) through the captured-graph plan
+    route: every MST slot, slot pattern, remaining capacity and Fenwick node
+    must equal the oracle's bit for bit."""
+    import torch
+
+    g, mst_c, pat_c = ref
+    R.reset()
+    R.plan_set(sofs, sids)
+    M = R.plan_slots
+    mst = torch.empty(M, dtype=torch.int64, device=f"cuda:{R.device}")
+    pat = torch.empty(M, dtype=torch.int32, device=f"cuda:{R.device}")
+    R.route_plan(mst, pat, graph=True)
+    R.sync()
+    same = (np.array_equal(mst.cpu().numpy(), mst_c) and np.array_equal(pat.cpu().numpy(), pat_c)
+            and np.array_equal(R.capr(), g.capr())
+            and np.array_equal(R.fenwick().view(np.uint32), g.fenwick().view(np.uint32)))
+    if not same:
+        raise SystemExit("the GPU route of the CPU sample differs from the oracle")
+    return f"bit-exact on {len(sids)} nets ({len(sofs) - 1} batches, {M} MST slots, all GCELLs and Fenwick nodes)"
 
 
 def run_reference(args, rank):
@@ -404,12 +433,14 @@ def main():
     d2h = M * 8 + M * 4 + 40 * (len(bofs) - 1)
 
     cpu = None
+    parity = None
     if rank == 0:
         sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
         nthreads = os.cpu_count() or 1
-        v_cpu, dt = time_oracle(d, ofs, pins, sofs, sids, nthreads)
+        v_cpu, dt, ref = time_oracle(d, ofs, pins, sofs, sids, nthreads, keep=True)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"every {stride}th batch of the plan ({nsel} batches, {len(sids)} nets, {dt:.1f} s)"}
+        parity = sample_parity(R, sofs, sids, ref)
 
     if dist:
         dist.barrier()
@@ -432,6 +463,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": replicas.whole_job_rate(n_nets, e2e_t, world), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
+        "parity": parity,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "quality": {"plain": {"overflow": q["overflow"], "overflow_cells": q["overflow_cells"], "demand": q["demand"],

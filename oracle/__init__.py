@@ -36,6 +36,7 @@ _SIG = {
     "gro_commit": (_I, [_P, _P, _P, _P, _I32, _P, _P, _P]),
     "gro_route_batch": (_I, [_P, _P, _P, _P, _I32, _P, _P, _P, _P, _P, _I]),
     "gro_route_batches": (_I, [_P, _P, _P, _P, _P, _I32, _P, _P, _I]),
+    "gro_count_oob_pairs": (None, [_P, _P, _P, _P, _I32, _P]),
 }
 _lib = None
 
@@ -153,6 +154,16 @@ class Grid:
         rc = lib().gro_route_batches(self._h, _p(pin_ofs), _p(pins), _p(ids), _p(batch_ofs), len(batch_ofs) - 1,
                                      _p(mst), _p(mp), nthreads)
         return rc, mst[:M], mp[:M]
+
+    def count_oob_pairs(self, pin_ofs, pins, net_ids):
+        """(pairs, pattern evaluations) for which the reference's L-pattern
+        kernel reads a second-via layer v2 == Z past the grid (odd Z)."""
+        pin_ofs = np.ascontiguousarray(pin_ofs, dtype=np.int64)
+        pins = np.ascontiguousarray(pins, dtype=np.int32)
+        ids = np.ascontiguousarray(net_ids, dtype=np.int32)
+        out = np.zeros(2, dtype=np.int64)
+        lib().gro_count_oob_pairs(self._h, _p(pin_ofs), _p(pins), _p(ids), len(ids), _p(out))
+        return int(out[0]), int(out[1])
 
 
 def batch_pairs(pin_ofs, pins, net_ids) -> np.ndarray:

@@ -239,6 +239,40 @@ int64_t gro_batch_pairs(const int64_t *pin_ofs, const int32_t *pins, const int32
     return id;
 }
 
+/* Pairs whose L patterns the reference evaluates with a second-via layer
+ * v2 == Z, past the top layer: bit_util.hpp:157-164 computes v2 = via1 odd ?
+ * 2v : 2v+1 with no v2 < DZ guard, so with odd Z every even via1 >= 2 and
+ * v = ceil(Z/2)-1 reach v2 = Z whenever both x and y differ (bth_diff), and
+ * the kernel then reads point and wire costs of layer Z out of bounds. The
+ * oracle treats those patterns as invalid. out[0] = such pairs, out[1] =
+ * such (pair, pattern) evaluations, over the nets listed. */
+void gro_count_oob_pairs(const gro_grid *g, const int64_t *pin_ofs, const int32_t *pins, const int32_t *net_ids,
+                         int32_t n_nets, int64_t out[2]) {
+    const int Z2 = (g->Z + 1) / 2;
+    int per_pair = 0;
+    for (int via1 = 1; via1 < g->Z; via1++)
+        for (int v = 0; v < Z2; v++) {
+            const int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
+            per_pair += via2 != 0 && via2 >= g->Z;
+        }
+    int64_t pairs = 0;
+    for (int32_t i = 0; i < n_nets && per_pair > 0; i++) {
+        const int64_t o = pin_ofs[net_ids[i]];
+        const int n = (int)(pin_ofs[net_ids[i] + 1] - o);
+        for (int j = 0; j < n; j++) {
+            int zj, xj, yj;
+            gro_dec(g, pins[o + j], &zj, &xj, &yj);
+            for (int k = 0; k < j; k++) {
+                int zk, xk, yk;
+                gro_dec(g, pins[o + k], &zk, &xk, &yk);
+                pairs += xj != xk && yj != yk;
+            }
+        }
+    }
+    out[0] = pairs;
+    out[1] = pairs * per_pair;
+}
+
 /* ---------------------------------------------------------------- Boruvka */
 
 /* order-preserving key of a float cost: ties on cost fall to the pair id */

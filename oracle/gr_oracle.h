@@ -75,6 +75,12 @@ void gro_lpattern(const gro_grid *g, const int32_t *pairs, int64_t n_pairs,
 int64_t gro_batch_pairs(const int64_t *pin_ofs, const int32_t *pins,
                         const int32_t *net_ids, int32_t n_nets, int32_t *pairs);
 
+/* pairs (out[0]) and pattern evaluations (out[1]) that the reference's
+ * L-pattern kernel makes with a second-via layer v2 == Z (odd Z only;
+ * bit_util.hpp:157-164 has no v2 < DZ guard) over the listed nets */
+void gro_count_oob_pairs(const gro_grid *g, const int64_t *pin_ofs, const int32_t *pins,
+                         const int32_t *net_ids, int32_t n_nets, int64_t out[2]);
+
 /* Boruvka of one net of n pins over w[n(n-1)/2]; writes n slots (edges then
  * -1), returns number of rounds or -1 on failure */
 int gro_brvsk_net(int n, const float *w, int64_t local_id, int64_t *slots, float *dist);

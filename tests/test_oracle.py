@@ -211,3 +211,27 @@ def test_golden_design_fixture():
     assert mp.tolist() == fx["mst_pat"]
     assert g.demand().tolist() == fx["demand"]
     assert int(g.fenwick().view(np.uint32).astype(np.uint64).sum()) == fx["fenwick_u32_sum"]
+
+
+def test_count_oob_pairs_matches_a_direct_count():
+    """The odd-Z count (pairs whose pins differ in x and y, each with the
+    patterns whose second via would be layer Z) against numpy on a small
+    design; zero for even Z."""
+    rng = np.random.default_rng(11)
+    for Z, per in ((9, 4), (5, 2), (10, 0), (4, 0)):
+        X, Y = 30, 20
+        g = oracle.Grid(X, Y, Z, np.ones(X * Y * Z, np.int32))
+        nets = [np.sort(rng.choice(X * Y * 2, size=int(n), replace=False)).astype(np.int32)
+                for n in rng.integers(2, 15, size=40)]
+        ofs = np.cumsum([0] + [len(q) for q in nets]).astype(np.int64)
+        pins = np.concatenate(nets)
+        ids = rng.permutation(len(nets)).astype(np.int32)
+        want = 0
+        for q in nets:
+            dec = []
+            for e in q:
+                z, r = divmod(int(e), X * Y)
+                dec.append((r // Y, r % Y) if z & 1 else (r % X, r // X))
+            want += sum(1 for j in range(len(q)) for k in range(j) if dec[j][0] != dec[k][0] and dec[j][1] != dec[k][1])
+        got = g.count_oob_pairs(ofs, pins, ids)
+        assert got == ((want, per * want) if per else (0, 0)), (Z, got, want)
