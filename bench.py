@@ -61,28 +61,30 @@ def net_bytes(d, ofs, pins, total_demand):
 def kernel_units(ofs, ids, committed):
     """Algorithmic units and bytes of one route step per profiled kernel kind:
     k_lpat reads two pins and writes a cost and a pattern per pair (14 B);
-    k_mark reads a slot and its pair's pattern and writes the slot's pattern
-    (14 B); Boruvka reads the net's pair costs and writes its slots and cost
-    sum (4 P + 8 n + 4 B); k_track_commit moves 16 B per committed GCELL
-    (capacity and Fenwick leaf, each read and written)."""
+    the tree kernels read the net's pair costs, write its slots and the
+    slots' patterns and read those from the pair patterns (4 P + 14 n B per
+    net; they also mark the trees' GCELLs); k_track_commit moves 16 B per
+    committed GCELL (capacity and Fenwick leaf, each read and written)."""
     n = np.diff(ofs)[ids].astype(np.int64)
     P = n * (n - 1) // 2
     big, mid = n > 32, (n > 2) & (n <= 32)
     return {
         "k_lpat": (int(P.sum()), 14 * int(P.sum())),
-        "k_mark": (int(n.sum()), 14 * int(n.sum())),
-        "k_mst_large": (int(P[big].sum()), int((4 * P + 8 * n + 4)[big].sum())),
-        "k_mst_warp": (int(P[mid].sum()), int((4 * P + 8 * n + 4)[mid].sum())),
+        "k_mst_large": (int(P[big].sum()), int((4 * P + 14 * n)[big].sum())),
+        "k_mst_warp": (int(P[mid].sum()), int((4 * P + 14 * n)[mid].sum())),
         "k_track_commit": (int(committed), 16 * int(committed)),
     }
 
 
-def learned_quality(d, R, mst, pat, n_batches, dims):
-    """Quality of the design routed with the lookahead cost, when the package
-    ships a network for this layer count (lookahead_z<Z>.npy with its
-    lookahead_z<Z>.json report naming beta and the prediction interval);
-    the time of a second, warm learned route (identical to the first) is
-    reported beside it (not part of `value`)."""
+def learned_quality(d, R, mst, pat, n_batches, dims, steps, warmup):
+    """The learned-lookahead route of the same design, when the package ships
+    a network for this layer count (lookahead_z<Z>.npy with its
+    lookahead_z<Z>.json naming the mode and beta): the whole route -- the
+    network's forward pass every `every` batches, the cost switch, the
+    Fenwick rebuilds and every batch -- as one captured CUDA graph
+    (gr_route_plan_lookahead), timed with CUDA events like `value`, at the
+    prediction interval of 64 batches and at the network's own interval, with
+    the routed design's quality. Not part of `value`."""
     import torch
 
     from iitmglobalrouter_b200 import lookahead
@@ -91,20 +93,36 @@ def learned_quality(d, R, mst, pat, n_batches, dims):
     if not base.with_suffix(".npy").exists():
         return None
     rep = json.loads(base.with_suffix(".json").read_text())
-    beta, every, mode = float(rep["beta"]), int(rep["every"]), rep.get("mode", "demand")
+    beta, mode = float(rep["beta"]), rep.get("mode", "demand")
     net = lookahead.LookaheadNet(2 * dims["Z"], dims["Z"], dims["Y"], dims["X"], hidden=rep["hidden"],
                                  n_layers=rep["layers"])
     net.set_params(np.load(base.with_suffix(".npy")))
-    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta, mode=mode)  # warm-up
-    first = mst.cpu().numpy()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    lookahead.route_lookahead(R, net, mst, pat, n_batches, every=every, beta=beta, mode=mode)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    assert np.array_equal(mst.cpu().numpy(), first), "the learned route is not deterministic"
-    out = lookahead.quality(d, R, mst, pat)
-    out.update(beta=beta, every=every, mode=mode, route_ms=dt * 1e3, weights=base.with_suffix(".npy").name)
+    stream = torch.cuda.ExternalStream(R.stream, device=mst.device)
+    out = {"beta": beta, "mode": mode, "weights": base.with_suffix(".npy").name}
+    for every in sorted({64, int(rep["every"])}, reverse=True):
+        for _ in range(warmup):
+            R.route_lookahead_plan(net, every, beta, mode, mst, pat, graph=True)
+        R.sync()
+        first = mst.cpu().numpy()
+        times = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            R.route_lookahead_plan(net, every, beta, mode, mst, pat, graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        R.sync()
+        net.check()
+        assert np.array_equal(mst.cpu().numpy(), first), "the learned route is not deterministic"
+        # quality of the learned routes' result: the demand is read after a
+        # route with the lookahead cost (the graph ends with the plain cost's
+        # trees rebuilt, the demand stays)
+        q = lookahead.quality(d, R, mst, pat)
+        ms = statistics.median(times)
+        q.update(every=every, route_ms=ms, value=d.dims["n_nets"] / (ms / 1e3), unit=UNIT, graph=True)
+        out[f"every_{every}"] = q
+    net.close()
     R.reset()
     return out
 
@@ -366,7 +384,7 @@ def main():
     if not replicas.replicas_agree(replicas.digest(mst_h, pat_h, demand), dist, dev):
         raise SystemExit("replicas routed the design differently")
     wl, vias = d.write_routes(os.devnull, mst_h, pat_h, merge=True, rseg=True, ppatch=True, threads=8)
-    learned = learned_quality(d, R, mst, pat, len(bofs) - 1, dims)
+    learned = learned_quality(d, R, mst, pat, len(bofs) - 1, dims, args.steps, args.warmup)
     learned_c2 = learned_quality_small()
 
     # per-kernel breakdown: one profiled step (events around each launch)

@@ -90,6 +90,9 @@ SIGNATURES = {
     "gr_cnn_get_params": (_I, [_P, _P]),
     "gr_cnn_set_params": (_I, [_P, _P]),
     "gr_cnn_forward": (_I, [_P, _P, _P]),
+    "gr_cnn_forward_async": (_I, [_P, _P, _P, _P]),
+    "gr_cnn_check": (_I, [_P]),
+    "gr_route_plan_lookahead": (_I, [_P, _P, C.c_int32, C.c_float, _I, _P, _P, _I, _P]),
     "gr_cnn_grads": (_I, [_P, _P, _P, _P, _P]),
     "gr_cnn_train_step": (_I, [_P, _P, _P, C.c_float, _P]),
     "gr_cnn_gemm_test": (_I, [_I, _I, _I, _P, _P, _P, _I]),

@@ -40,7 +40,6 @@ struct BatchInfo {  // one batch of a plan
     int32_t max_pins;
     int32_t n2, nm, nl;  // nets of 2 pins, 3..32 pins, more
     int32_t nmid;        // of the nl larger nets, those up to kMstMidPins pins (listed first)
-    int64_t s2 = 0, sm = 0, smid = 0;  // MST slots of the 2-pin, 3..32-pin and mid classes
 };
 
 struct GraphCache {
@@ -61,7 +60,6 @@ struct gr_ctx {
     float *d_fen = nullptr, *d_lut = nullptr;
     uint32_t *d_mark = nullptr, *d_status = nullptr;
     DevBuf mat;                            // per-CTA pair-cost matrices of the largest nets
-    int32_t *d_list_count = nullptr;
     std::vector<int32_t> h_cap0;
     // design
     int32_t n_nets = 0;
@@ -90,10 +88,7 @@ struct gr_ctx {
     float *d_pred = nullptr;
     float la_beta = 0.0f;
     bool la_on = false;
-    // tracks that gained marked cells in a batch: bitmap, list of first cells
-    uint32_t *d_tbits = nullptr;
-    int32_t *d_tlist = nullptr;
-    int32_t n_tracks = 0;
+    int32_t n_tracks = 0;                      // routing tracks: rows of even layers, columns of odd ones
     int track_cap = 0;                         // marked cells per track compacted in shared memory
     int32_t *d_gpos = nullptr;                 // CSIZE scratch for tracks beyond track_cap (long tracks only)
     float *d_gdel = nullptr;
@@ -103,12 +98,11 @@ struct gr_ctx {
     int64_t plan_nets = 0, plan_slots = 0;
     int64_t plan_max_pairs = 0, plan_max_tab = 0, plan_max_nets = 0;
     GraphCache graph;
+    GraphCache la_graph;  // the learned route of the plan (route_lookahead_impl)
     int64_t launches = 0;
     int mst_smem_max = 0;
     int32_t plan_max_pins = 0;  // largest net of the uploaded plan
     DevBuf plan_ids, plan_bofs, plan_pb;  // device plan builder: inputs, per-batch totals and an error flag
-    DevBuf plan_slot0, slot_net;          // per batch its first MST slot; per plan slot its net
-    DevBuf slot_ord;                      // per batch its slots in class order (k_plan_slot_order)
     bool h_nxy_valid = false;             // h_nxy mirrors d_nxy (copied when a host-built descriptor needs it)
     int *d_queue = nullptr;  // k_mst_queue: next item, CTAs finished (zero between launches)
     int tune[GR_TUNE_PARAMS] = {1024, 1024, 1024, 129, 0, 0};  // GR_TUNE_* values (best measured on B200, Z = 10)
@@ -271,14 +265,6 @@ int fill_desc(const gr_ctx *c, const int32_t *ids, int32_t n, void *dst, int64_t
     bi.nm = nm;
     bi.nl = n - n2 - nm;
     bi.nmid = nmid;
-    bi.s2 = 2 * (int64_t)n2;
-    bi.sm = 0;
-    bi.smid = 0;
-    for (int32_t i = 0; i < n; i++) {
-        const int32_t k = npin[i];
-        if (k != 2 && k <= kMstWarpPins) bi.sm += k;
-        else if (k > kMstWarpPins && k <= kMstMidPins) bi.smid += k;
-    }
     bi.first = first;
     bi.n = n;
     bi.n_pairs = P;
@@ -298,9 +284,6 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
     v.nm = bi.nm;
     v.nl = bi.nl;
     v.nmid = bi.nmid;
-    v.s2 = bi.s2;
-    v.sm = bi.sm;
-    v.smid = bi.smid;
     return v;
 }
 
@@ -328,9 +311,10 @@ int mst_cluster_size(int n, int from_pins = 0) {
 // ------------------------------------------------------------------ stages
 
 // mst (may be null): also write the trees of the batch's 2-pin nets (and
-// their dist), so that launch_mst can skip k_mst_pin2
+// their dist), so that launch_mst can skip k_mst_pin2, and mark their paths
+// when mo.mark is set
 int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat, float2 *tab, cudaStream_t s,
-                      int64_t *mst = nullptr, float *dist = nullptr) {
+                      int64_t *mst = nullptr, float *dist = nullptr, MarkOut mo = MarkOut{}) {
     if (v.n_tab > 0) {
         int pi = prof_begin(c, s);
         k_qtable<<<grid_for(c, v.n_tab, 16), kThreads, 0, s>>>(c->g, v, coords(c), c->d_fen, tab);
@@ -353,20 +337,20 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
     case ZV:                                                                                              \
         if (split == 4)                                                                                   \
             k_lpat_zs<ZV, 4><<<grid_s, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, \
-                                                         ppat, mst, dist);                                \
+                                                         ppat, mst, dist, mo, c->d_status);               \
         else if (split == 2)                                                                              \
             k_lpat_zs<ZV, 2><<<grid_s, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, \
-                                                         ppat, mst, dist);                                \
+                                                         ppat, mst, dist, mo, c->d_status);               \
         else                                                                                              \
             k_lpat_z<ZV><<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat, \
-                                                   mst, dist);                                            \
+                                                   mst, dist, mo, c->d_status);                           \
         break;
         switch (c->g.Z) {
             GR_LPAT_Z(3) GR_LPAT_Z(4) GR_LPAT_Z(5) GR_LPAT_Z(6) GR_LPAT_Z(7) GR_LPAT_Z(8) GR_LPAT_Z(9)
             GR_LPAT_Z(10) GR_LPAT_Z(11) GR_LPAT_Z(12) GR_LPAT_Z(13) GR_LPAT_Z(14) GR_LPAT_Z(15) GR_LPAT_Z(16)
             default:
                 k_lpat_batch<<<grid, kThreads, 0, s>>>(c->g, v, c->d_pins, coords(c), c->d_fen, tab, pcost, ppat,
-                                                       mst, dist);
+                                                       mst, dist, mo, c->d_status);
         }
 #undef GR_LPAT_Z
         prof_end(c, s, pi, GR_K_LPAT);
@@ -375,38 +359,33 @@ int launch_lpat_batch(gr_ctx *c, const BatchView &v, float *pcost, int16_t *ppat
     return GR_OK;
 }
 
-// What the marking needs besides the batch view: the pair patterns and where
-// the slots' patterns go.
-struct MarkArgs {
-    const int16_t *ppat;
-    int32_t *mst_pat;
-};
+// where a batch's marking goes (the context's bitmap), for pair patterns
+// ppat and slot patterns mst_pat (may be null)
+MarkOut mark_out(const gr_ctx *c, const int16_t *ppat, int32_t *mst_pat) {
+    return MarkOut{c->d_mark, mst_pat, ppat, c->d_pins};
+}
 
-// k_mark7 over slots k0..k1-1 (entries of v.slot_ord when set) on stream s
-int launch_mark(gr_ctx *c, const BatchView &v, const int64_t *mst, const MarkArgs &mk, int64_t k0, int64_t k1,
-                cudaStream_t s) {
-    if (k1 <= k0) return GR_OK;
+// k_mark over the batch's slots (trees that did not come from this
+// context's tree kernels)
+int launch_mark(gr_ctx *c, const BatchView &v, const int64_t *mst, const MarkOut &mo, cudaStream_t s) {
+    if (v.n_nodes <= 0) return GR_OK;
     int pi = prof_begin(c, s);
-    k_mark7<<<grid_for(c, (k1 - k0) * 32, 8), kThreads, 0, s>>>(c->g, v, c->d_pins, mst, mk.ppat, mk.mst_pat, c->d_mark,
-                                                               c->d_tbits, c->d_tlist, c->d_list_count, c->d_status,
-                                                               v.slot_ord, k0, k1);
+    k_mark<<<grid_for(c, v.n_nodes, 8), kThreads, 0, s>>>(c->g, v, mst, mo, c->d_status);
     prof_end(c, s, pi, GR_K_MARK);
     GR_CK(cudaGetLastError());
     return GR_OK;
 }
 
-// mk (plans only, v.slot_ord set, the track count already cleared and the
-// 2-pin trees already written): each size class's slots are marked on the
-// class's stream right after its trees, so the marking of the small classes
-// overlaps the Boruvka of the large nets and only the largest class's marking
-// remains on the batch's critical path
+// mo.mark set: every tree kernel marks the GCELLs of the trees it builds
+// (and writes the slots' patterns), right after building each one
 int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, float *dist, cudaStream_t s,
-               bool pin2_done = false, const MarkArgs *mk = nullptr) {
+               bool pin2_done = false, MarkOut mo = MarkOut{}) {
     if (v.n <= 0) return GR_OK;
     if (c->tune[GR_TUNE_MST_QUEUE]) {
         if (v.n2 > 0 && !pin2_done) {
             int pi = prof_begin(c, s);
-            k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
+            k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(c->g, v, pcost, mst, dist, mo,
+                                                                          c->d_status);
             prof_end(c, s, pi, GR_K_MST);
         }
         const int items = v.nl + (v.nm + kQueueWarps - 1) / kQueueWarps;
@@ -427,7 +406,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         vv.max_pins = maxn;
         int pi = prof_begin(c, s);
         k_mst_queue<<<blocks, kQueueThreads, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
-                                                      (int64_t)maxn * maxn, c->d_queue);
+                                                      (int64_t)maxn * maxn, c->d_queue, mo);
         prof_end(c, s, pi, GR_K_MST_LARGE);
         GR_CK(cudaGetLastError());
         return GR_OK;
@@ -443,19 +422,15 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
     };
     if (v.n2 > 0 && !pin2_done) {
         int pi = prof_begin(c, s);
-        k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(v, pcost, mst, dist);
+        k_mst_pin2<<<(v.n2 + kThreads - 1) / kThreads, kThreads, 0, s>>>(c->g, v, pcost, mst, dist, mo,
+                                                                          c->d_status);
         prof_end(c, s, pi, GR_K_MST);
     }
     if (v.nm > 0) {
         cudaStream_t s0 = side(0);
         int pi = prof_begin(c, s0);
-        k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s0>>>(c->g, v, pcost, mst, dist, c->d_status);
+        k_mst_warp<<<(v.nm + 7) / 8, 256, 0, s0>>>(c->g, v, pcost, mst, dist, c->d_status, mo);
         prof_end(c, s0, pi, GR_K_MST_WARP);
-    }
-    if (mk) {  // 2-pin trees exist since the L-pattern kernel: marked beside every class's Boruvka
-        int rc = launch_mark(c, v, mst, *mk, 0, v.s2, s);
-        if (!rc && v.sm > 0) rc = launch_mark(c, v, mst, *mk, v.s2, v.s2 + v.sm, side(0));
-        if (rc) return rc;
     }
     // larger nets: 128-thread CTAs up to 128 pins, 512-thread CTAs above. A
     // net's full cost matrix sits in the CTA's shared memory when it fits, is
@@ -488,10 +463,10 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
             cfg.numAttrs = 1;
             if (cs == 4)
                 GR_CK(cudaLaunchKernelEx(&cfg, k_mst_cluster<4>, c->g, vv, (const float *)pcost, mst, dist,
-                                         c->d_status, first, cnt));
+                                         c->d_status, first, cnt, mo));
             else
                 GR_CK(cudaLaunchKernelEx(&cfg, k_mst_cluster<8>, c->g, vv, (const float *)pcost, mst, dist,
-                                         c->d_status, first, cnt));
+                                         c->d_status, first, cnt, mo));
         } else {
             const bool in_smem = mst_mat_in_smem(maxn);
             const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
@@ -502,15 +477,10 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
                 if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
                 gmat = (uint32_t *)c->mat.p;
             }
-            k_mst_large<<<blocks, c->tune[part ? GR_TUNE_MST_BIG_THREADS : GR_TUNE_MST_MID_THREADS], sm, sp>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
-                                                              (int64_t)maxn * maxn, first, cnt);
+            k_mst_large<<<blocks, c->tune[part ? GR_TUNE_MST_BIG_THREADS : GR_TUNE_MST_MID_THREADS], sm, sp>>>(
+                c->g, vv, pcost, mst, dist, c->d_status, gmat, (int64_t)maxn * maxn, first, cnt, mo);
         }
         prof_end(c, sp, pi, GR_K_MST_LARGE);
-        if (mk) {
-            const int64_t k0 = v.s2 + v.sm + (part ? v.smid : 0);
-            int rc = launch_mark(c, v, mst, *mk, k0, part ? v.n_nodes : k0 + v.smid, sp);
-            if (rc) return rc;
-        }
     }
     for (int i = 0; i < 3; i++)
         if (used[i]) {
@@ -530,24 +500,20 @@ constexpr int kTrackCapMax = 256;
 
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
 
-// count_cleared: an L-pattern kernel of this batch already set the track count to 0
-// marked: launch_mst already marked the batch's slots
+// marked: the tree kernels already marked the batch's slots
 int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16_t *ppat, int32_t *mst_pat,
-                  cudaStream_t s, bool count_cleared = false, bool marked = false) {
+                  cudaStream_t s, bool marked = false) {
     if (v.n_nodes <= 0) return GR_OK;
     if (!marked) {
-        if (!count_cleared) GR_CK(cudaMemsetAsync(c->d_list_count, 0, sizeof(int32_t), s));
-        BatchView va = v;
-        va.slot_ord = nullptr;  // all slots in batch order
-        int rc = launch_mark(c, va, mst, MarkArgs{ppat, mst_pat}, 0, v.n_nodes, s);
+        int rc = launch_mark(c, v, mst, mark_out(c, ppat, mst_pat), s);
         if (rc) return rc;
     }
     int pi = prof_begin(c, s);
     int64_t blocks = ((int64_t)c->n_tracks + kTrackWarps - 1) / kTrackWarps;
     if (blocks > (int64_t)c->sm_count * 8) blocks = (int64_t)c->sm_count * 8;
     k_track_commit<<<(int)blocks, kTrackWarps * 32, track_smem(c->track_cap), s>>>(
-        c->g, c->d_tlist, c->d_list_count, c->d_mark, c->d_tbits, c->d_capr, c->d_dlut, c->d_fen, c->d_gpos,
-        c->d_gdel, c->track_cap, c->la_on ? c->d_pred : nullptr, c->la_beta);
+        c->g, c->n_tracks, c->d_mark, c->d_capr, c->d_dlut, c->d_fen, c->d_gpos, c->d_gdel, c->track_cap,
+        c->la_on ? c->d_pred : nullptr, c->la_beta);
     prof_end(c, s, pi, GR_K_FEN_UPDATE);
     GR_CK(cudaGetLastError());
     return GR_OK;
@@ -622,18 +588,16 @@ int upload_batch(gr_ctx *c, const int32_t *ids, int32_t n, BatchInfo &bi, BatchV
     return GR_OK;
 }
 
+// One batch: L-pattern (which also settles and marks the 2-pin nets), the
+// trees of the other nets (each marked by the kernel that builds it), then
+// the commit of every marked GCELL.
 int route_one(gr_ctx *c, const BatchView &v, int64_t *mst, int32_t *mst_pat, float *dist, float *pcost,
               int16_t *ppat, cudaStream_t s) {
     int rc;
-    BatchView vl = v;  // the L-pattern kernel also clears the marking's track count
-    vl.zero_count = c->d_list_count;
-    if ((rc = launch_lpat_batch(c, vl, pcost, ppat, (float2 *)c->tab.p, s, mst, dist))) return rc;
-    // per-class marking on the Boruvka streams needs the class-ordered slot
-    // list of a plan and the track count cleared by the L-pattern kernel
-    const bool split = v.slot_ord && v.n_pairs > 0 && !c->tune[GR_TUNE_MST_QUEUE];
-    const MarkArgs mk{ppat, mst_pat};
-    if ((rc = launch_mst(c, v, pcost, mst, dist, s, true, split ? &mk : nullptr))) return rc;
-    return launch_commit(c, v, mst, ppat, mst_pat, s, v.n_pairs > 0, split);
+    const MarkOut mo = mark_out(c, ppat, mst_pat);
+    if ((rc = launch_lpat_batch(c, v, pcost, ppat, (float2 *)c->tab.p, s, mst, dist, mo))) return rc;
+    if ((rc = launch_mst(c, v, pcost, mst, dist, s, true, mo))) return rc;
+    return launch_commit(c, v, mst, ppat, mst_pat, s, true);
 }
 
 void free_buf(DevBuf &b) {
@@ -645,6 +609,11 @@ void free_buf(DevBuf &b) {
 void drop_graph(gr_ctx *c) {
     if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
     c->graph = GraphCache{};
+}
+
+void drop_la_graph(gr_ctx *c) {
+    if (c->la_graph.exec) cudaGraphExecDestroy(c->la_graph.exec);
+    c->la_graph = GraphCache{};
 }
 
 // Fenwick trees from the current capacities, with the plain or the lookahead cost
@@ -733,12 +702,10 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     c->track_cap = (X > Y ? X : Y) < kTrackCapMax ? (X > Y ? X : Y) : kTrackCapMax;
     // capr is read in aligned 32-cell words: pad it to a whole last word
     if (cudaMalloc(&c->d_cap0, cell4) || cudaMalloc(&c->d_capr, cell4 + 128) || cudaMalloc(&c->d_fen, cell4) ||
-        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_list_count, 16) || cudaMalloc(&c->d_status, 16) ||
+        cudaMalloc(&c->d_mark, words * 4) || cudaMalloc(&c->d_status, 16) ||
         cudaMalloc(&c->d_queue, 16) ||
         cudaMalloc(&c->d_lut, sizeof(float) * (kLutMax - kLutMin + 1)) ||
         cudaMalloc(&c->d_dlut, sizeof(float) * (kLutMax - kLutMin + 2)) ||
-        cudaMalloc(&c->d_tbits, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2)) ||
-        cudaMalloc(&c->d_tlist, sizeof(int32_t) * (size_t)(c->n_tracks + 1)) ||
         (c->track_cap < (X > Y ? X : Y) &&
          (cudaMalloc(&c->d_gpos, sizeof(int32_t) * (size_t)csize) ||
           cudaMalloc(&c->d_gdel, sizeof(float) * (size_t)csize)))) {
@@ -756,8 +723,7 @@ int gr_create(gr_ctx **out, int device, int X, int Y, int Z, const int32_t *h_ca
     if (cudaMemcpyAsync(c->d_lut, lut.data(), sizeof(float) * lut.size(), cudaMemcpyHostToDevice, s0) ||
         cudaMemcpyAsync(c->d_cap0, h_cap, cell4, cudaMemcpyHostToDevice, s0) ||
         cudaMemsetAsync(c->d_mark, 0, words * 4, s0) || cudaMemsetAsync(c->d_status, 0, 16, s0) ||
-        cudaMemsetAsync(c->d_list_count, 0, 16, s0) || cudaMemsetAsync(c->d_queue, 0, 16, s0) ||
-        cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s0))
+        cudaMemsetAsync(c->d_queue, 0, 16, s0))
         return fail(GR_ERR_CUDA);
     // A function attribute holds for the whole process, not this context:
     // set it to the most any context launches with, so that a context for a
@@ -796,21 +762,19 @@ int gr_destroy(gr_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graph(c);
+    drop_la_graph(c);
     cudaFree(c->d_cap0);
     cudaFree(c->d_capr);
     cudaFree(c->d_fen);
     cudaFree(c->d_lut);
     cudaFree(c->d_dlut);
     cudaFree(c->d_pred);
-    cudaFree(c->d_tbits);
-    cudaFree(c->d_tlist);
     cudaFree(c->d_gpos);
     cudaFree(c->d_gdel);
     cudaFree(c->d_mark);
     cudaFree(c->d_status);
     cudaFree(c->d_queue);
     free_buf(c->mat);
-    cudaFree(c->d_list_count);
     cudaFree(c->d_pins);
     cudaFree(c->d_pxy);
     cudaFree(c->d_cx);
@@ -836,9 +800,6 @@ int gr_destroy(gr_ctx *c) {
     free_buf(c->plan_ids);
     free_buf(c->plan_bofs);
     free_buf(c->plan_pb);
-    free_buf(c->plan_slot0);
-    free_buf(c->slot_net);
-    free_buf(c->slot_ord);
     for (int i = 0; i < 3; i++) {
         if (c->side[i]) cudaStreamSynchronize(c->side[i]), cudaStreamDestroy(c->side[i]);
         if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
@@ -856,7 +817,6 @@ int gr_reset(gr_ctx *c, void *stream) {
     cudaStream_t s = pick(c, stream);
     GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * c->csize, cudaMemcpyDeviceToDevice, s));
     GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(c->csize / 32 + 2), s));
-    GR_CK(cudaMemsetAsync(c->d_tbits, 0, sizeof(uint32_t) * (size_t)(c->n_tracks / 32 + 2), s));
     GR_CK(cudaMemsetAsync(c->d_queue, 0, 16, s));
     return rebuild_fenwick(c, s);
 }
@@ -1071,9 +1031,6 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
         bi.nm = q.nm;
         bi.nmid = q.nmid;
         bi.nl = bi.n - q.n2 - q.nm;
-        bi.s2 = q.s2;
-        bi.sm = q.sm;
-        bi.smid = q.smid;
         if ((rc = check_mst_smem(c, bi.max_pins))) return rc;
     }
     for (int32_t b = 0; b < n_batches; b++) {
@@ -1088,26 +1045,6 @@ int gr_plan_set(gr_ctx *c, int32_t n_batches, const int64_t *h_batch_ofs, const 
     c->plan_max_pins = plan_max_pins;
     if ((rc = ensure_mst_scratch(c, plan_max_pins, c->stream))) return rc;
     if ((rc = ensure_scratch(c, mp, mt, mn, c->stream))) return rc;
-    // slot -> net map for the marking kernel (saves it a search per slot)
-    if (n_batches > 0 && slot > 0) {
-        std::vector<int64_t> s0(n_batches);
-        for (int32_t b = 0; b < n_batches; b++) s0[b] = plan[b].slot0;
-        if ((rc = ensure(c->plan_slot0, sizeof(int64_t) * n_batches, c->stream)) ||
-            (rc = ensure(c->slot_net, sizeof(int32_t) * (size_t)slot, c->stream)))
-            return rc;
-        GR_CK(cudaMemcpyAsync(c->plan_slot0.p, s0.data(), sizeof(int64_t) * n_batches, cudaMemcpyHostToDevice,
-                              c->stream));
-        k_plan_slots<<<n_batches, 256, 0, c->stream>>>((const int64_t *)c->plan_bofs.p, (const int64_t *)c->plan_slot0.p,
-                                                      all.npin, all.node_ofs, (int32_t *)c->slot_net.p);
-        c->launches++;
-        // slots in class order: each size class is marked on its own stream
-        if ((rc = ensure(c->slot_ord, sizeof(int32_t) * (size_t)slot, c->stream))) return rc;
-        k_plan_slot_order<<<n_batches, 1024, 0, c->stream>>>((const int64_t *)c->plan_bofs.p,
-                                                            (const int64_t *)c->plan_slot0.p, all.npin, all.node_ofs,
-                                                            all.order, (int32_t *)c->slot_ord.p);
-        c->launches++;
-        GR_CK(cudaGetLastError());
-    }
     GR_CK(cudaStreamSynchronize(c->stream));
     c->plan = std::move(plan);
     c->plan_nets = total;
@@ -1138,23 +1075,9 @@ int gr_plan_check(gr_ctx *c) {
         BatchInfo hb{};
         if ((rc = fill_desc(c, ids.data() + bi.first, bi.n, host.data(), total, bi.first, hb))) return rc;
         bad |= hb.n_pairs != bi.n_pairs || hb.n_nodes != bi.n_nodes || hb.n_tab != bi.n_tab ||
-               hb.max_pins != bi.max_pins || hb.n2 != bi.n2 || hb.nm != bi.nm || hb.nl != bi.nl || hb.nmid != bi.nmid ||
-               hb.s2 != bi.s2 || hb.sm != bi.sm || hb.smid != bi.smid;
+               hb.max_pins != bi.max_pins || hb.n2 != bi.n2 || hb.nm != bi.nm || hb.nl != bi.nl || hb.nmid != bi.nmid;
     }
     bad |= memcmp(dev.data(), host.data(), bytes - 64) != 0;
-    // the class-ordered slot list against the host descriptor's order
-    if (!bad && c->plan_slots > 0 && c->slot_ord.p) {
-        std::vector<int32_t> so((size_t)c->plan_slots);
-        GR_CK(cudaMemcpy(so.data(), c->slot_ord.p, sizeof(int32_t) * so.size(), cudaMemcpyDeviceToHost));
-        for (const BatchInfo &bi : c->plan) {
-            const BatchView hv = view_of(host.data(), total, bi.first, bi.n);
-            int64_t k = bi.slot0;
-            for (int32_t p = 0; p < bi.n && !bad; p++) {
-                const int32_t i = hv.order[p];
-                for (int32_t j = 0; j < hv.npin[i]; j++) bad |= so[(size_t)k++] != (int32_t)hv.node_ofs[i] + j;
-            }
-        }
-    }
     return bad ? GR_ERR_DEVICE : GR_OK;
 }
 
@@ -1170,11 +1093,10 @@ std::vector<uint64_t> graph_sig(const gr_ctx *c, int32_t b0, int32_t b1, const v
                                 cudaStream_t s, const void *h_mst, const void *h_pat) {
     std::vector<uint64_t> v;
     auto P = [&](const void *p) { v.push_back((uint64_t)(uintptr_t)p); };
-    const void *const ptrs[] = {mst, pat, (const void *)s, h_mst, h_pat, c->plan_desc.p, c->slot_net.p, c->slot_ord.p, c->pcost.p,
+    const void *const ptrs[] = {mst, pat, (const void *)s, h_mst, h_pat, c->plan_desc.p, c->pcost.p,
                           c->ppat.p, c->tab.p, c->dist.p, c->mat.p, (const void *)c->d_pins, (const void *)c->d_pxy,
                           (const void *)c->d_cx, (const void *)c->d_cy, (const void *)c->d_fen, (const void *)c->d_capr,
-                          (const void *)c->d_mark, (const void *)c->d_tbits, (const void *)c->d_tlist,
-                          (const void *)c->d_list_count, (const void *)c->d_status, (const void *)c->d_dlut,
+                          (const void *)c->d_mark, (const void *)c->d_status, (const void *)c->d_dlut,
                           (const void *)c->d_gpos, (const void *)c->d_gdel, (const void *)c->d_pred,
                           (const void *)c->d_queue};
     for (const void *p : ptrs) P(p);
@@ -1187,7 +1109,7 @@ std::vector<uint64_t> graph_sig(const gr_ctx *c, int32_t b0, int32_t b1, const v
     for (int32_t b = b0; b < b1; b++) {
         const BatchInfo &bi = c->plan[b];
         const int64_t f[] = {bi.first, (int64_t)bi.n, bi.n_pairs, bi.n_nodes, bi.n_tab, bi.slot0, (int64_t)bi.max_pins,
-                             (int64_t)bi.n2, (int64_t)bi.nm, (int64_t)bi.nl, (int64_t)bi.nmid, bi.s2, bi.sm, bi.smid};
+                             (int64_t)bi.n2, (int64_t)bi.nm, (int64_t)bi.nl, (int64_t)bi.nmid};
         for (int64_t x : f) v.push_back((uint64_t)x);
     }
     return v;
@@ -1206,9 +1128,7 @@ int route_plan_impl(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int
     auto issue = [&]() -> int {
         for (int32_t b = b0; b < b1; b++) {
             const BatchInfo &bi = c->plan[b];
-            BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
-            if (c->slot_net.p) v.slot_net = (const int32_t *)c->slot_net.p + bi.slot0;
-            if (c->slot_ord.p) v.slot_ord = (const int32_t *)c->slot_ord.p + bi.slot0;
+            const BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
             // no per-net tree costs: a plan returns trees and patterns only
             int rc = route_one(c, v, d_mst_edges + bi.slot0, d_mst_pat ? d_mst_pat + bi.slot0 : nullptr, nullptr,
                                (float *)c->pcost.p, (int16_t *)c->ppat.p, s);
@@ -1259,6 +1179,102 @@ int route_plan_impl(gr_ctx *c, int32_t b0, int32_t b1, int64_t *d_mst_edges, int
     }
     GR_CK(cudaGraphLaunch(gc.exec, s));
     c->launches += gc.launches;
+    return GR_OK;
+}
+
+// The learned route of the whole plan from reset on stream s: before every
+// `every` batches, the network predicts from the current state (features
+// x 1/16) the demand still to come (output x 16; in GR_LA_EXCESS mode its
+// part beyond the remaining capacity), the GCELL cost becomes
+// exp(-0.5 (cap_remaining - beta pred)) and the Fenwick trees are rebuilt;
+// at the end the plain cost and its trees are restored. Every step is on the
+// device (the network's forward pass included), so with GR_PLAN_GRAPH the
+// whole route is one captured CUDA graph, replayed while its signature holds.
+int route_lookahead_impl(gr_ctx *c, gr_cnn *cnn, int32_t every, float beta, int mode, int64_t *mst, int32_t *pat,
+                         int flags, cudaStream_t s) {
+    const int64_t n = c->csize;
+    const int32_t nb = (int32_t)c->plan.size();
+    int rc;
+    if ((rc = ensure(c->la_feat, sizeof(float) * 2 * n, s)) || (rc = ensure(c->la_out, sizeof(float) * 2 * n, s)) ||
+        (rc = ensure_mst_scratch(c, c->plan_max_pins, s)))
+        return rc;
+    if (!c->d_pred && cudaMalloc(&c->d_pred, sizeof(float) * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        return GR_ERR_NOMEM;
+    }
+    // any graph of the plain route holds the cost mode it was captured with
+    drop_graph(c);
+    float *feat = (float *)c->la_feat.p, *out = (float *)c->la_out.p, *pred = out + n;
+    auto issue = [&]() -> int {
+        int r;
+        c->la_on = false;
+        c->la_beta = 0.0f;
+        GR_CK(cudaMemcpyAsync(c->d_capr, c->d_cap0, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, s));
+        GR_CK(cudaMemsetAsync(c->d_mark, 0, sizeof(uint32_t) * (size_t)(n / 32 + 2), s));
+        GR_CK(cudaMemsetAsync(c->d_queue, 0, 16, s));
+        if (beta == 0.0f && (r = rebuild_fenwick(c, s))) return r;
+        for (int32_t b0 = 0; b0 < nb; b0 += every) {
+            const int32_t b1 = b0 + every < nb ? b0 + every : nb;
+            if (beta > 0.0f) {
+                k_features<<<grid_for(c, n, 16), kThreads, 0, s>>>(c->g, (int)n, c->d_cap0, c->d_capr, 1.0f / 16.0f,
+                                                                   feat);
+                c->launches++;
+                if ((r = gr_cnn_forward_async(cnn, feat, out, s))) return r;
+                const int64_t gz = (int64_t)c->g.Z * c->g.X * c->g.Y;
+                k_la_pred<<<grid_for(c, gz, 16), kThreads, 0, s>>>((int)gz, out, feat, mode == GR_LA_EXCESS, pred);
+                k_pred_to_cells<<<grid_for(c, n, 16), kThreads, 0, s>>>(c->g, (int)n, pred, c->d_pred);
+                c->launches += 2;
+                GR_CK(cudaGetLastError());
+                c->la_on = true;
+                c->la_beta = beta;
+                if ((r = rebuild_fenwick(c, s))) return r;
+            }
+            for (int32_t b = b0; b < b1; b++) {
+                const BatchInfo &bi = c->plan[b];
+                const BatchView v = make_view(c->plan_desc.p, c->plan_nets, bi);
+                if ((r = route_one(c, v, mst + bi.slot0, pat ? pat + bi.slot0 : nullptr, nullptr, (float *)c->pcost.p,
+                                   (int16_t *)c->ppat.p, s)))
+                    return r;
+            }
+        }
+        c->la_on = false;  // the plain cost and its trees back
+        c->la_beta = 0.0f;
+        return rebuild_fenwick(c, s);
+    };
+    if (!(flags & GR_PLAN_GRAPH)) return issue();
+    GraphCache &gc = c->la_graph;
+    std::vector<uint64_t> sig = graph_sig(c, 0, nb, mst, pat, s, nullptr, nullptr);
+    uint32_t beta_bits;
+    memcpy(&beta_bits, &beta, 4);
+    for (uint64_t x : {(uint64_t)(uintptr_t)cnn, (uint64_t)every, (uint64_t)beta_bits, (uint64_t)mode,
+                       (uint64_t)(uintptr_t)c->la_feat.p, (uint64_t)(uintptr_t)c->la_out.p})
+        sig.push_back(x);
+    if (!(gc.exec && gc.sig == sig)) {
+        drop_la_graph(c);
+        const int64_t before = c->launches;
+        cudaGraph_t graph = nullptr;
+        GR_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int r = issue();
+        const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (r) {
+            if (graph) cudaGraphDestroy(graph);
+            return r;
+        }
+        if (ce != cudaSuccess) return GR_ERR_CUDA;
+        const cudaError_t ie = cudaGraphInstantiate(&gc.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            gc.exec = nullptr;
+            return GR_ERR_CUDA;
+        }
+        gc.sig = std::move(sig);
+        gc.launches = c->launches - before;
+        c->launches = before;
+    }
+    GR_CK(cudaGraphLaunch(gc.exec, s));
+    c->launches += gc.launches;
+    c->la_on = false;  // the graph ends with the plain cost restored
+    c->la_beta = 0.0f;
     return GR_OK;
 }
 
@@ -1386,46 +1402,38 @@ int gr_set_lookahead(gr_ctx *c, const float *d_pred, float beta, void *stream) {
     return rebuild_fenwick(c, s);
 }
 
-int gr_route_design_lookahead_host(gr_ctx *c, gr_cnn *cnn, int32_t every, float beta, int mode,
-                                   int64_t *h_mst_edges, int32_t *h_mst_pat) {
-    if (!c || !cnn || !h_mst_edges || every < 1 || !(beta >= 0.0f) || (mode != GR_LA_DEMAND && mode != GR_LA_EXCESS))
+int gr_route_plan_lookahead(gr_ctx *c, gr_cnn *cnn, int32_t every, float beta, int mode, int64_t *d_mst_edges,
+                            int32_t *d_mst_pat, int flags, void *stream) {
+    if (!c || !cnn || !d_mst_edges || every < 1 || !(beta >= 0.0f) || (mode != GR_LA_DEMAND && mode != GR_LA_EXCESS))
         return GR_ERR_ARG;
     if (c->plan.empty()) return GR_ERR_STATE;
     int dev = -1, cin = 0, cout = 0, H = 0, W = 0;
     int rc = gr_cnn_info(cnn, &dev, &cin, &cout, &H, &W);
     if (rc) return rc;
     if (dev != c->device || cin != 2 * c->g.Z || cout != c->g.Z || H != c->g.Y || W != c->g.X) return GR_ERR_ARG;
-    const int64_t slots = c->plan_slots, n = c->csize;
-    const int32_t nb = (int32_t)c->plan.size();
+    return route_lookahead_impl(c, cnn, every, beta, mode, d_mst_edges, d_mst_pat, flags, pick(c, stream));
+}
+
+int gr_route_design_lookahead_host(gr_ctx *c, gr_cnn *cnn, int32_t every, float beta, int mode,
+                                   int64_t *h_mst_edges, int32_t *h_mst_pat) {
+    if (!c || !h_mst_edges) return GR_ERR_ARG;
+    if (c->plan.empty()) return GR_ERR_STATE;
+    const int64_t slots = c->plan_slots;
+    int rc;
     if ((rc = ensure(c->out_mst, sizeof(int64_t) * (slots + 1), c->stream)) ||
-        (rc = ensure(c->out_pat, sizeof(int32_t) * (slots + 1), c->stream)) ||
-        (rc = ensure(c->la_feat, sizeof(float) * 2 * n, c->stream)) ||
-        (rc = ensure(c->la_out, sizeof(float) * 2 * n, c->stream)))
+        (rc = ensure(c->out_pat, sizeof(int32_t) * (slots + 1), c->stream)))
         return rc;
     int64_t *mst = (int64_t *)c->out_mst.p;
     int32_t *pat = (int32_t *)c->out_pat.p;
-    float *feat = (float *)c->la_feat.p, *out = (float *)c->la_out.p, *pred = out + n;
-    if ((rc = gr_set_lookahead(c, nullptr, 0.0f, nullptr)) || (rc = gr_reset(c, nullptr))) return rc;
-    for (int32_t b0 = 0; b0 < nb && !rc; b0 += every) {
-        const int32_t b1 = b0 + every < nb ? b0 + every : nb;
-        if (beta > 0.0f) {
-            if ((rc = gr_features(c, feat, 1.0f / 16.0f, nullptr))) break;
-            GR_CK(cudaStreamSynchronize(c->stream));  // the network reads on its own stream
-            if ((rc = gr_cnn_forward(cnn, feat, out))) break;
-            k_la_pred<<<grid_for(c, n, 16), kThreads, 0, c->stream>>>((int)n, out, feat, mode == GR_LA_EXCESS, pred);
-            GR_CK(cudaGetLastError());
-            if ((rc = gr_set_lookahead(c, pred, beta, nullptr))) break;
-        }
-        rc = gr_route_plan(c, b0, b1, mst, pat, 0, nullptr);
-    }
+    rc = gr_route_plan_lookahead(c, cnn, every, beta, mode, mst, pat, GR_PLAN_GRAPH, nullptr);
     if (!rc) {
         GR_CK(cudaMemcpyAsync(h_mst_edges, mst, sizeof(int64_t) * slots, cudaMemcpyDeviceToHost, c->stream));
         if (h_mst_pat)
             GR_CK(cudaMemcpyAsync(h_mst_pat, pat, sizeof(int32_t) * slots, cudaMemcpyDeviceToHost, c->stream));
     }
     const int sr = gr_sync(c);
-    const int lr = gr_set_lookahead(c, nullptr, 0.0f, nullptr);
-    return rc ? rc : (sr ? sr : lr);
+    const int cr = gr_cnn_check(cnn);
+    return rc ? rc : (sr ? sr : cr);
 }
 
 int gr_tune_set(gr_ctx *c, int param, int value) {
@@ -1442,6 +1450,7 @@ int gr_tune_set(gr_ctx *c, int param, int value) {
     if (c->tune[param] != value) {
         GR_CK(cudaStreamSynchronize(c->stream));
         drop_graph(c);  // a captured plan holds the old launch shapes
+        drop_la_graph(c);
         c->tune[param] = value;
     }
     return GR_OK;
@@ -1535,10 +1544,10 @@ static __device__ __align__(256) unsigned char g_brvsk_scratch[kStaticScratchByt
 namespace {
 
 // Pair and slot offsets of a batch from its pin counts: one CTA of 1024
-// threads, each scanning a contiguous chunk, 64-bit sums throughout.
+// threads, each scanning a contiguous chunk, 64-bit sums throughout. (The
+// nets' processing order is uploaded beside the pin counts.)
 __global__ void __launch_bounds__(1024) k_static_desc(int32_t n, const int32_t *__restrict__ npin,
-                                                      int32_t *__restrict__ order, int64_t *__restrict__ pair_ofs,
-                                                      int64_t *__restrict__ node_ofs) {
+                                                      int64_t *__restrict__ pair_ofs, int64_t *__restrict__ node_ofs) {
     const unsigned FULL = 0xffffffffu;
     __shared__ long long wp[32], wn[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
@@ -1586,7 +1595,6 @@ __global__ void __launch_bounds__(1024) k_static_desc(int32_t n, const int32_t *
         const long long k = npin[i];
         pair_ofs[i] = P;
         node_ofs[i] = N;
-        order[i] = i;
         P += k * (k - 1) / 2;
         N += k;
     }
@@ -1634,12 +1642,24 @@ extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, cons
     if (n_nets < 0 || n_nets > kStaticMaxNets) return GR_ERR_ARG;
     if (n_nets == 0) return GR_OK;
     if (!h_npin || !d_pair_cost || !d_mst_edges) return GR_ERR_ARG;
-    int maxn = 0;
+    // nets whose pair-cost matrix fits in shared memory first, in batch
+    // order, then the larger ones: each group gets its own launch, so the
+    // small nets never queue behind the few CTAs the array's matrices allow
+    int max_small = 0, max_large = 0;
+    std::vector<int32_t> order((size_t)n_nets);
+    int32_t n_small = 0;
     for (int32_t i = 0; i < n_nets; i++) {
         if (h_npin[i] < 0) return GR_ERR_ARG;
         if (h_npin[i] > kStaticMaxPins) return GR_ERR_NET_TOO_LARGE;
-        maxn = h_npin[i] > maxn ? h_npin[i] : maxn;
+        if (mst_mat_in_smem(h_npin[i])) {
+            order[n_small++] = i;
+            max_small = h_npin[i] > max_small ? h_npin[i] : max_small;
+        } else {
+            max_large = h_npin[i] > max_large ? h_npin[i] : max_large;
+        }
     }
+    for (int32_t i = 0, k = n_small; i < n_nets; i++)
+        if (!mst_mat_in_smem(h_npin[i])) order[k++] = i;
     int dev = 0;
     GR_CK(cudaGetDevice(&dev));
     StaticDev sd;
@@ -1647,38 +1667,40 @@ extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, cons
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     uint32_t *st = d_status ? d_status : (uint32_t *)(sd.base + kSsStatus);
-    int32_t *npin = (int32_t *)(sd.base + kSsNpin), *order = (int32_t *)(sd.base + kSsOrder);
+    int32_t *npin = (int32_t *)(sd.base + kSsNpin), *dorder = (int32_t *)(sd.base + kSsOrder);
     int64_t *pair_ofs = (int64_t *)(sd.base + kSsPairOfs), *node_ofs = (int64_t *)(sd.base + kSsNodeOfs);
     GR_CK(cudaMemsetAsync(sd.base + kSsStatus, 0, sizeof(uint32_t), s));
     GR_CK(cudaMemcpyAsync(npin, h_npin, sizeof(int32_t) * (size_t)n_nets, cudaMemcpyHostToDevice, s));
-    k_static_desc<<<1, 1024, 0, s>>>(n_nets, npin, order, pair_ofs, node_ofs);
+    GR_CK(cudaMemcpyAsync(dorder, order.data(), sizeof(int32_t) * (size_t)n_nets, cudaMemcpyHostToDevice, s));
+    k_static_desc<<<1, 1024, 0, s>>>(n_nets, npin, pair_ofs, node_ofs);
     GR_CK(cudaGetLastError());
     BatchView v{};
     v.n = n_nets;
     v.npin = npin;
     v.pair_ofs = pair_ofs;
     v.node_ofs = node_ofs;
-    v.order = order;
-    v.max_pins = maxn;
-    // k_mst_large for every net: the matrix in shared memory when the largest
-    // net's fits, else one matrix per CTA in the array (as many CTAs as the
-    // array holds, at most one per SM)
-    const bool in_smem = mst_mat_in_smem(maxn);
-    const size_t mat = (size_t)maxn * maxn * sizeof(float);
-    const size_t smem = mst_smem(maxn) + (in_smem ? mat : 0);
-    int blocks;
-    uint32_t *gmat = nullptr;
-    if (in_smem) {
-        blocks = n_nets < sd.sms * 8 ? n_nets : sd.sms * 8;
-    } else {
-        const size_t fit = (kStaticScratchBytes - kSsMat) / mat;
-        blocks = (int)(fit < (size_t)sd.sms ? fit : (size_t)sd.sms);
-        blocks = n_nets < blocks ? n_nets : blocks;
-        gmat = (uint32_t *)(sd.base + kSsMat);
+    v.order = dorder;
+    // k_mst_large: the small nets with their matrices in shared memory on up
+    // to 8 CTAs per SM; the larger ones with one matrix per CTA in the array
+    // (as many CTAs as it holds, at most one per SM)
+    if (n_small > 0) {
+        v.max_pins = max_small;
+        const size_t smem = mst_smem(max_small) + (size_t)max_small * max_small * sizeof(float);
+        const int blocks = n_small < sd.sms * 8 ? n_small : sd.sms * 8;
+        k_mst_large<<<blocks, max_small <= kMstMidPins ? 128 : 512, smem, s>>>(
+            GridC{}, v, d_pair_cost, d_mst_edges, d_net_dist, st, nullptr, 0, 0, n_small, MarkOut{});
+        GR_CK(cudaGetLastError());
     }
-    k_mst_large<<<blocks, maxn <= kMstMidPins ? 128 : 512, smem, s>>>(GridC{}, v, d_pair_cost, d_mst_edges,
-                                                                      d_net_dist, st, gmat, (int64_t)maxn * maxn,
-                                                                      0, n_nets);
-    GR_CK(cudaGetLastError());
+    if (n_small < n_nets) {
+        v.max_pins = max_large;
+        const size_t mat = (size_t)max_large * max_large * sizeof(float);
+        const size_t fit = (kStaticScratchBytes - kSsMat) / mat;
+        int blocks = (int)(fit < (size_t)sd.sms ? fit : (size_t)sd.sms);
+        blocks = n_nets - n_small < blocks ? n_nets - n_small : blocks;
+        k_mst_large<<<blocks, 512, mst_smem(max_large), s>>>(GridC{}, v, d_pair_cost, d_mst_edges, d_net_dist, st,
+                                                             (uint32_t *)(sd.base + kSsMat), (int64_t)max_large * max_large,
+                                                             n_small, n_nets - n_small, MarkOut{});
+        GR_CK(cudaGetLastError());
+    }
     return GR_OK;
 }

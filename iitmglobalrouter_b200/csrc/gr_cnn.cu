@@ -643,9 +643,8 @@ bool conv_tc_fits(const gr_cnn *c, int l) {
     return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16), c->cin[l]) <= kConvSmemMax;
 }
 
-int forward(gr_cnn *c) {
+int forward(gr_cnn *c, cudaStream_t s) {
     const int M = c->H * c->W;
-    cudaStream_t s = c->stream;
     for (int l = 0; l < c->n_layers; l++) {
         const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
         if (conv_tc_fits(c, l)) {
@@ -849,10 +848,27 @@ int gr_cnn_forward(gr_cnn *c, const float *d_in, float *d_out) {
     if (!c || !d_in || !d_out) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, c->stream);
     if (rc) return rc;
     CN_CK(cudaMemcpyAsync(d_out, c->act[c->n_layers], sizeof(float) * M * c->cout[c->n_layers - 1],
                           cudaMemcpyDeviceToDevice, c->stream));
+    return finish(c);
+}
+
+int gr_cnn_forward_async(gr_cnn *c, const float *d_in, float *d_out, void *stream) {
+    if (!c || !d_in || !d_out) return GR_ERR_ARG;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    const int64_t M = (int64_t)c->H * c->W;
+    CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, s));
+    int rc = forward(c, s);
+    if (rc) return rc;
+    CN_CK(cudaMemcpyAsync(d_out, c->act[c->n_layers], sizeof(float) * M * c->cout[c->n_layers - 1],
+                          cudaMemcpyDeviceToDevice, s));
+    return GR_OK;
+}
+
+int gr_cnn_check(gr_cnn *c) {
+    if (!c) return GR_ERR_ARG;
     return finish(c);
 }
 
@@ -860,7 +876,7 @@ int gr_cnn_grads(gr_cnn *c, const float *d_in, const float *d_target, float *h_g
     if (!c || !d_in || !d_target) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, c->stream);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     if (h_grads)
@@ -873,7 +889,7 @@ int gr_cnn_train_step(gr_cnn *c, const float *d_in, const float *d_target, float
     if (!c || !d_in || !d_target || !(lr > 0.0f)) return GR_ERR_ARG;
     const int64_t M = (int64_t)c->H * c->W;
     CN_CK(cudaMemcpyAsync(c->act[0], d_in, sizeof(float) * M * c->cin[0], cudaMemcpyDeviceToDevice, c->stream));
-    int rc = forward(c);
+    int rc = forward(c, c->stream);
     if (!rc) rc = backward(c, d_target);
     if (rc) return rc;
     c->adam_t++;

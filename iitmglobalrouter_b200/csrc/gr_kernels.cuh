@@ -12,9 +12,11 @@
 //   k_mst_warp     Boruvka of 3..32-pin nets, one warp each
 //   k_mst_large    Boruvka of larger nets, one CTA each
 //   k_mst_cluster  Boruvka of nets whose cost matrix needs a 4- or 8-CTA cluster
-//   k_mark7        GCELLs of every MST edge, batch-deduped, and the tracks
-//                  they lie on                                (mst_bit_commit.hpp:81-235)
-//   k_track_commit per touched track: demand += 1 per marked cell and the
+//                  (the L-pattern and tree kernels also mark the GCELLs of
+//                  every MST edge they settle, batch-deduped in a bitmap,
+//                  mst_bit_commit.hpp:81-235; k_mark does it for trees
+//                  built elsewhere)
+//   k_track_commit per routing track: demand += 1 per marked cell and the
 //                  Fenwick node updates, one owner per node   (bit_util.hpp:75-90)
 #pragma once
 #include <cooperative_groups.h>
@@ -40,17 +42,7 @@ struct BatchView {
     int32_t max_pins;
     int32_t n2, nm, nl;       // sizes of the three classes in `order`
     int32_t nmid;             // of the nl larger nets, the first nmid have at most 128 pins
-    const int32_t *slot_net;  // [n_nodes] net of each MST slot (plans only; null: found by search)
-    const int32_t *slot_ord;  // [n_nodes] the batch's slots, nets in `order` (plans only, else null)
-    int64_t s2, sm, smid;     // MST slots of the 2-pin, 3..32-pin and 33..128-pin classes (plans only)
-    int32_t *zero_count;      // set to 0 by the L-pattern kernel (the marking's track count), or null
 };
-
-// the L-pattern kernels clear the batch's touched-track count for the marking
-// kernel that follows them (one memset node less per batch)
-__device__ __forceinline__ void lpat_clear_count(const BatchView &bv) {
-    if (bv.zero_count && blockIdx.x == 0 && threadIdx.x == 0) *bv.zero_count = 0;
-}
 
 // Per design pin (indexed like the pin array): the pin's index into its net's
 // sorted distinct x and y lists, packed (xi << 16) | yi; and the lists
@@ -236,20 +228,6 @@ __global__ void k_fen_init(GridC g, int csize, const int32_t *__restrict__ capr,
     }
 }
 
-// The plan's slot -> net map: slot slot0[b] + node_ofs[i] + j (pin j of net i
-// of batch b) holds i. One CTA per batch, one thread per net.
-__global__ void k_plan_slots(const int64_t *__restrict__ bofs, const int64_t *__restrict__ slot0,
-                             const int32_t *__restrict__ npin, const int64_t *__restrict__ node_ofs,
-                             int32_t *__restrict__ slot_net) {
-    const int64_t first = bofs[blockIdx.x];
-    const int n = (int)(bofs[blockIdx.x + 1] - first);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        int32_t *dst = slot_net + slot0[blockIdx.x] + node_ofs[first + i];
-        const int k = npin[first + i];
-        for (int j = 0; j < k; j++) dst[j] = i;
-    }
-}
-
 // Routing tracks (a row of an even layer, a column of an odd layer) are
 // numbered layer by layer: layer z starts at track_first(z).
 __device__ __forceinline__ int track_first(const GridC &g, int z) { return ((z + 1) >> 1) * g.Y + (z >> 1) * g.X; }
@@ -303,7 +281,6 @@ __global__ void __launch_bounds__(128) k_fen_tracks(GridC g, int n_tracks, int l
 // batch.
 struct PlanBatch {  // per-batch totals for the host's launch shapes
     int64_t n_pairs, n_nodes, n_tab;
-    int64_t s2, sm, smid;  // MST slots of the 2-pin, 3..warp_pins and ..mid_pins classes
     int32_t max_pins, n2, nm, nmid;
 };
 
@@ -375,7 +352,6 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
     __syncthreads();
     // pass 1: offsets, class counts, largest net
     int64_t P = 0, Mn = 0, T = 0;
-    int64_t k0 = 0, k1 = 0, k2 = 0;  // this thread's MST slots per class
     int c0 = 0, c1 = 0, c2 = 0;
     for (int base = 0; base < n; base += blockDim.x) {
         const int i = base + tid;
@@ -400,15 +376,10 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
         Mn += tb;
         T += tc;
         const int q = i < n ? cls(k) : -1;
-        k0 += q == 0 ? k : 0;
-        k1 += q == 1 ? k : 0;
-        k2 += q == 2 ? k : 0;
         c0 += __syncthreads_count(q == 0);
         c1 += __syncthreads_count(q == 1);
         c2 += __syncthreads_count(q == 2);
     }
-    int64_t S0, S1, S2;
-    block_excl_scan3(k0, k1, k2, S0, S1, S2, wsum);
     // pass 2: stable partition by class
     int run[4] = {0, c0, c0 + c1, c0 + c1 + c2};
     for (int base = 0; base < n; base += blockDim.x) {
@@ -439,9 +410,6 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
         pb.n_pairs = P;
         pb.n_nodes = Mn;
         pb.n_tab = T;
-        pb.s2 = S0;
-        pb.sm = S1;
-        pb.smid = S2;
         pb.max_pins = s_max;
         pb.n2 = c0;
         pb.nm = c1;
@@ -450,37 +418,132 @@ __global__ void __launch_bounds__(1024) k_plan_batches(const int64_t *__restrict
     }
 }
 
-// The plan's class-ordered slot list: batch b's slots, net by net in the
-// batch's `order` (2-pin nets, then 3..32 pins, 33..128, larger), each net's
-// slots in turn; entries are slot indices relative to the batch. The marking
-// of one size class then covers a contiguous range of the list. One CTA
-// (1024 threads) per batch.
-__global__ void __launch_bounds__(1024) k_plan_slot_order(const int64_t *__restrict__ bofs,
-                                                          const int64_t *__restrict__ slot0,
-                                                          const int32_t *__restrict__ npin,
-                                                          const int64_t *__restrict__ node_ofs,
-                                                          const int32_t *__restrict__ order,
-                                                          int32_t *__restrict__ slot_ord) {
-    __shared__ int64_t wsum[32][3];
-    const int64_t first = bofs[blockIdx.x];
-    const int n = (int)(bofs[blockIdx.x + 1] - first);
-    int32_t *dst = slot_ord + slot0[blockIdx.x];
-    int64_t run = 0;
-    for (int base = 0; base < n; base += blockDim.x) {
-        const int p = base + threadIdx.x;
-        int i = 0;
-        int64_t k = 0, z1 = 0, z2 = 0, t0, t1, t2;
-        if (p < n) {
-            i = order[first + p];
-            k = npin[first + i];
+// ---------------------------------------------------------------- marking
+// The GCELLs of one committed edge (mst_bit_commit.hpp:36-67, 209-231): a
+// layer change covers its interior layers, a wire its inclusive span. Each
+// cell is visited once: V::span(first id, count) for a wire (ids contiguous
+// along the track), V::cell(id) for a via cell. Only stacked pins (same x
+// and y) can revisit a cell -- the two layer changes and the one-cell wire
+// share a column -- so that case visits the union of their layers.
+__device__ __forceinline__ uint64_t layer_interior(int a, int b) {
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    if (hi - lo < 2) return 0;
+    return ((1ull << hi) - 1) & ~((1ull << (lo + 1)) - 1);
+}
+
+template <class V>
+__device__ __forceinline__ bool walk_edge(const GridC &g, int z1, int x1, int y1, int z2, int x2, int y2, int cpat,
+                                          V &vis) {
+    const int via1 = cpat / g.Z2, v = cpat % g.Z2;
+    const bool bth = (x1 != x2 && y1 != y2);
+    const int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
+    if (cpat < 0 || via1 < 1 || via1 >= g.Z || (bth && via2 != 0 && via2 >= g.Z)) return false;
+    // The reference's marking kernel walks the first wire also for the
+    // threads of the first layer change's d interior cells, whose local
+    // index is then -d..-1 (the one call not guarded by tid >= 0,
+    // mst_bit_commit.hpp:216): they mark the d cells below the wire's lower
+    // end -- cell ids first-d .. first-1 of the wire's track, or the end of
+    // the previous track when that end is at coordinate 0.
+    const int d = z1 == via1 ? 0 : (z1 < via1 ? via1 - z1 : z1 - via1) - 1;
+    if (x1 == x2 && y1 == y2) {
+        uint64_t m = layer_interior(z1, via1) | (1ull << via1) | layer_interior(via1, z2);
+        while (m) {
+            const int i = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            vis.cell(enc(g, i, x1, y1));
         }
-        block_excl_scan3(k, z1, z2, t0, t1, t2, wsum);  // k: this net's first position in the list
-        if (p < n) {
-            const int32_t s = (int32_t)node_ofs[first + i];
-            const int cnt = npin[first + i];
-            for (int j = 0; j < cnt; j++) dst[run + k + j] = s + j;
+        if (d > 0) vis.span(enc(g, via1, x1, y1) - d, d);
+        return true;
+    }
+    auto via = [&](int za, int zb) {
+        const int lo = za < zb ? za : zb, hi = za < zb ? zb : za;
+        for (int i = lo + 1; i < hi; i++) vis.cell(enc(g, i, x1, y1));
+    };
+    auto wire = [&](int z) {
+        if (z & 1) {
+            const int lo = min(y1, y2), hi = max(y1, y2);
+            vis.span(z * g.XY + x1 * g.Y + lo, hi - lo + 1);
+            y1 = y2;
+        } else {
+            const int lo = min(x1, x2), hi = max(x1, x2);
+            vis.span(z * g.XY + y1 * g.X + lo, hi - lo + 1);
+            x1 = x2;
         }
-        run += t0;
+    };
+    if (z1 != via1) {
+        via(z1, via1);
+        z1 = via1;
+    }
+    if (d > 0) vis.span(((z1 & 1) ? z1 * g.XY + x1 * g.Y + min(y1, y2) : z1 * g.XY + y1 * g.X + min(x1, x2)) - d, d);
+    wire(z1);
+    if (bth && via2 != 0 && z1 != via2) {
+        via(z1, via2);
+        z1 = via2;
+        wire(z1);
+    }
+    if (z1 != z2) via(z1, z2);
+    return x1 == x2 && y1 == y2;
+}
+
+// Where the marking of a batch's MST edges goes: one bit per GCELL in `mark`
+// (the commit then adds one unit of demand to every marked cell: a GCELL
+// gains at most one unit per batch, mst_bit_commit.hpp:36-67, 236-255), and
+// each MST slot's pattern in mst_pat (-1 for sentinels; may be null). ppat:
+// the batch's pair patterns; pins: the design's pins. mark == null: the
+// trees are built without marking (the brvsk_build boundary).
+struct MarkOut {
+    uint32_t *mark;
+    int32_t *mst_pat;
+    const int16_t *ppat;
+    const int32_t *pins;
+};
+
+// walk_edge visitor: ORs the path's GCELL bits into the bitmap. The old
+// words are not needed, so the ORs are fire-and-forget reductions.
+struct RedMark {
+    uint32_t *mark;
+    __device__ void cell(int32_t e) { atomicOr(mark + (e >> 5), 1u << (e & 31)); }
+    __device__ void span(int32_t e0, int cnt) {
+        const int32_t e1 = e0 + cnt - 1, w0 = e0 >> 5, w1 = e1 >> 5;
+        for (int32_t w = w0; w <= w1; w++) {
+            uint32_t m = 0xffffffffu;
+            if (w == w0) m &= 0xffffffffu << (e0 & 31);
+            if (w == w1) m &= 0xffffffffu >> (31 - (e1 & 31));
+            atomicOr(mark + w, m);
+        }
+    }
+};
+
+// Marks MST slot `slot` of the batch: the edge between pins u and v of batch
+// net `net` (v < 0: a sentinel). As in mst_bit_commit.hpp:81-105 the larger
+// pin index is the source, the pair's pattern the path (bit_util.hpp:134-180
+// walked by mst_bit_commit.hpp:147-235).
+__device__ __forceinline__ void mark_edge_slot(const GridC &g, const BatchView &bv, const MarkOut &mo, int net,
+                                               int64_t slot, int u, int v, uint32_t *status) {
+    if (v < 0) {
+        if (mo.mst_pat) mo.mst_pat[slot] = -1;
+        return;
+    }
+    const int n1 = u > v ? u : v, n2 = u > v ? v : u;
+    const int cpat = mo.ppat[bv.pair_ofs[net] + (int64_t)n1 * (n1 - 1) / 2 + n2];
+    if (mo.mst_pat) mo.mst_pat[slot] = cpat;
+    const int32_t *np = mo.pins + bv.pin_base[net];
+    int z1, x1, y1, z2, x2, y2;
+    dec(g, __ldg(np + n1), z1, x1, y1);
+    dec(g, __ldg(np + n2), z2, x2, y2);
+    RedMark rm{mo.mark};
+    if (!walk_edge(g, z1, x1, y1, z2, x2, y2, cpat, rm)) atomicOr(status, 0x2u);
+}
+
+// The recorded slots of one net, read back from `out` (written by the
+// calling threads before a barrier), marked by threads t0, t0 + stride, ...
+__device__ __forceinline__ void mark_net_slots(const GridC &g, const BatchView &bv, const MarkOut &mo, int net,
+                                               const int64_t *out, int n, int t0, int stride, uint32_t *status) {
+    const int64_t o = bv.node_ofs[net];
+    for (int s = t0; s < n; s += stride) {
+        const int64_t E = out[s];
+        mark_edge_slot(g, bv, mo, net, o + s, E < 0 ? -1 : (int)((E >> 15) & 0x7fff), E < 0 ? -1 : (int)(E & 0x7fff),
+                       status);
     }
 }
 
@@ -514,22 +577,32 @@ __global__ void k_qtable(GridC g, BatchView bv, Coords cd, const float *__restri
 
 // ---------------------------------------------------------------- L-pattern
 // A 2-pin net's tree is its single pair: written by the L-pattern kernels in
-// the fused route (same slots as k_mst_pin2: root 0 records (0, 1)).
-__device__ __forceinline__ void pin2_tree(const BatchView &bv, int net, float c, int64_t *__restrict__ mst,
-                                          float *__restrict__ dist) {
+// the fused route (same slots as k_mst_pin2: root 0 records (0, 1)), and its
+// path marked there (pin 1 at (z1, x1, y1) is the source, pattern cp).
+__device__ __forceinline__ void pin2_tree(const GridC &g, const BatchView &bv, const MarkOut &mo, int net, float c,
+                                          int cp, int z1, int x1, int y1, int z2, int x2, int y2,
+                                          int64_t *__restrict__ mst, float *__restrict__ dist, uint32_t *status) {
     if (!mst || bv.npin[net] != 2) return;
     const int64_t o = bv.node_ofs[net];
     mst[o] = ((int64_t)net << 30) | 1;
     mst[o + 1] = -1;
     if (dist) dist[net] = c;
+    if (mo.mark) {
+        if (mo.mst_pat) {
+            mo.mst_pat[o] = cp;
+            mo.mst_pat[o + 1] = -1;
+        }
+        RedMark rm{mo.mark};
+        if (!walk_edge(g, z1, x1, y1, z2, x2, y2, cp, rm)) atomicOr(status, 0x2u);
+    }
 }
 
 __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const int32_t *__restrict__ pins,
                                                     Coords cd, const float *__restrict__ fen,
                                                     const float2 *__restrict__ tab,
                                                     float *__restrict__ cost, int16_t *__restrict__ pat,
-                                                    int64_t *__restrict__ mst, float *__restrict__ dist) {
-    lpat_clear_count(bv);
+                                                    int64_t *__restrict__ mst, float *__restrict__ dist, MarkOut mo,
+                                                    uint32_t *status) {
     const int lane = threadIdx.x & 31;
     for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
          p0 += (int64_t)gridDim.x * blockDim.x) {
@@ -570,7 +643,7 @@ __global__ void __launch_bounds__(256) k_lpat_batch(GridC g, BatchView bv, const
         }
         cost[p] = c;
         pat[p] = (int16_t)cp;
-        pin2_tree(bv, net, c, mst, dist);
+        pin2_tree(g, bv, mo, net, c, cp, z1, x1, y1, z2, x2, y2, mst, dist, status);
     }
 }
 
@@ -769,10 +842,10 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
 // into a full symmetric n x n matrix M (shared memory when it fits, else this
 // CTA's global scratch) so that each pin's crossing scan is one coalesced row
 // read by a warp.
-__device__ __forceinline__ void mst_block_net(const BatchView &bv, const float *__restrict__ cost,
-                                              int64_t *__restrict__ mst, float *__restrict__ dist, uint32_t *status,
-                                              const MstArrays &a, uint32_t *M, int net, int *warp_sums,
-                                              int *s_total) {
+__device__ __forceinline__ void mst_block_net(const GridC &g, const BatchView &bv, const MarkOut &mo,
+                                              const float *__restrict__ cost, int64_t *__restrict__ mst,
+                                              float *__restrict__ dist, uint32_t *status, const MstArrays &a,
+                                              uint32_t *M, int net, int *warp_sums, int *s_total) {
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     const int n = bv.npin[net];
     const long long P = (long long)n * (n - 1) / 2;
@@ -820,12 +893,13 @@ __device__ __forceinline__ void mst_block_net(const BatchView &bv, const float *
         if (nrec != n - 1) atomicOr(status, 0x4u);
     }
     __syncthreads();
+    if (mo.mark) mark_net_slots(g, bv, mo, net, out, n, tid, B, status);  // the tree's slots, thread by thread
 }
 
 __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const float *__restrict__ cost,
                                                    int64_t *__restrict__ mst, float *__restrict__ dist,
                                                    uint32_t *status, uint32_t *__restrict__ gmat, int64_t gmat_stride,
-                                                   int first, int count) {
+                                                   int first, int count, MarkOut mo) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_total;
@@ -833,7 +907,7 @@ __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const
     const MstArrays a = MstArrays::carve(sm, maxn);
     uint32_t *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : (uint32_t *)a.end(maxn);
     for (int t = blockIdx.x; t < count; t += gridDim.x)
-        mst_block_net(bv, cost, mst, dist, status, a, M, bv.order[first + t], warp_sums, &s_total);
+        mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, bv.order[first + t], warp_sums, &s_total);
 }
 
 // Nets whose n x n matrix exceeds one CTA's shared memory: a cluster of CS
@@ -843,7 +917,7 @@ __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const
 template <int CS>
 __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, const float *__restrict__ cost,
                                                      int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                     uint32_t *status, int first, int count) {
+                                                     uint32_t *status, int first, int count, MarkOut mo) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_total;
@@ -907,7 +981,9 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
                 if (nrec != n - 1) atomicOr(status, 0x4u);
             }
         }
-        cl.sync();
+        cl.sync();  // rank 0's slots written (cluster-scope release / acquire)
+        // the tree's slots marked by every thread of the cluster
+        if (mo.mark) mark_net_slots(g, bv, mo, net, mst + bv.node_ofs[net], n, rank * B + tid, CS * B, status);
     }
 }
 
@@ -1023,8 +1099,8 @@ template <int ZC>
 __global__ void __launch_bounds__(256, 3) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
                                                 const float *__restrict__ fen, const float2 *__restrict__ tab,
                                                 float *__restrict__ cost, int16_t *__restrict__ pat,
-                                                int64_t *__restrict__ mst, float *__restrict__ dist) {
-    lpat_clear_count(bv);
+                                                int64_t *__restrict__ mst, float *__restrict__ dist, MarkOut mo,
+                                                uint32_t *status) {
     const int lane = threadIdx.x & 31;
     for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
          p0 += (int64_t)gridDim.x * blockDim.x) {
@@ -1051,7 +1127,7 @@ __global__ void __launch_bounds__(256, 3) k_lpat_z(GridC g, BatchView bv, const 
         }
         cost[p] = c;
         pat[p] = (int16_t)cp;
-        pin2_tree(bv, net, c, mst, dist);
+        pin2_tree(g, bv, mo, net, c, cp, z1, x1, y1, z2, x2, y2, mst, dist, status);
     }
 }
 
@@ -1074,8 +1150,7 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
                                                  Coords cd, const float *__restrict__ fen,
                                                  const float2 *__restrict__ tab, float *__restrict__ cost,
                                                  int16_t *__restrict__ pat, int64_t *__restrict__ mst,
-                                                 float *__restrict__ dist) {
-    lpat_clear_count(bv);
+                                                 float *__restrict__ dist, MarkOut mo, uint32_t *status) {
     static_assert(S == 2 || S == 4 || S == 8, "warps per pair group");
     __shared__ float sc[8][32];
     __shared__ int sp[8][32], sf[8][32];
@@ -1087,6 +1162,7 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
         float c = inf;
         int bp = -1, first = -1;
         int net = 0;
+        int z1 = 0, x1 = 0, y1 = 0, z2 = 0, x2 = 0, y2 = 0;
         if (p0 < bv.n_pairs) {  // warp-uniform
             net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
                                   p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
@@ -1094,7 +1170,6 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
                 int j, k;
                 pair_decode(p - bv.pair_ofs[net], j, k);
                 const int32_t *np = pins + bv.pin_base[net];
-                int z1, x1, y1, z2, x2, y2;
                 dec(g, __ldg(np + j), z1, x1, y1);
                 dec(g, __ldg(np + k), z2, x2, y2);
                 const int nxy = bv.nxy[net];
@@ -1134,7 +1209,7 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
             }
             cost[p] = bc;
             pat[p] = (int16_t)bbp;
-            pin2_tree(bv, net, bc, mst, dist);
+            pin2_tree(g, bv, mo, net, bc, bbp, z1, x1, y1, z2, x2, y2, mst, dist, status);
         }
         __syncthreads();
     }
@@ -1143,8 +1218,8 @@ __global__ void __launch_bounds__(256, 2) k_lpat_zs(GridC g, BatchView bv, const
 // ---------------------------------------------------------------- Boruvka, small nets
 // Nets of 2 pins: one thread each (the single pair is the tree; the
 // reference's first candidate root 0 records (0, 1)).
-__global__ void k_mst_pin2(BatchView bv, const float *__restrict__ cost, int64_t *__restrict__ mst,
-                           float *__restrict__ dist) {
+__global__ void k_mst_pin2(GridC g, BatchView bv, const float *__restrict__ cost, int64_t *__restrict__ mst,
+                           float *__restrict__ dist, MarkOut mo, uint32_t *status) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= bv.n2) return;
     const int i = bv.order[t];
@@ -1152,15 +1227,20 @@ __global__ void k_mst_pin2(BatchView bv, const float *__restrict__ cost, int64_t
     mst[o] = ((int64_t)i << 30) | 1;
     mst[o + 1] = -1;
     if (dist) dist[i] = cost[bv.pair_ofs[i]];
+    if (mo.mark) {
+        mark_edge_slot(g, bv, mo, i, o, 0, 1, status);
+        mark_edge_slot(g, bv, mo, i, o + 1, -1, -1, status);
+    }
 }
 
 // Nets of 3..32 pins: one warp each, pin = lane, the same per-round rule as
 // k_mst_large with the candidate forest resolved by shuffles. skey/scomp: 32
 // entries, sw: the net's pair costs (kMstWarpPins * (kMstWarpPins - 1) / 2),
 // all in this warp's shared memory.
-__device__ __forceinline__ void mst_warp_net(const BatchView &bv, const float *__restrict__ cost,
-                                             int64_t *__restrict__ mst, float *__restrict__ dist, uint32_t *status,
-                                             int i, unsigned long long *skey, int *scomp, float *sw, int lane) {
+__device__ __forceinline__ void mst_warp_net(const GridC &g, const BatchView &bv, const MarkOut &mo,
+                                             const float *__restrict__ cost, int64_t *__restrict__ mst,
+                                             float *__restrict__ dist, uint32_t *status, int i,
+                                             unsigned long long *skey, int *scomp, float *sw, int lane) {
     const unsigned FULL = 0xffffffffu;
     const int n = bv.npin[i];
     {
@@ -1227,20 +1307,24 @@ __device__ __forceinline__ void mst_warp_net(const BatchView &bv, const float *_
         if (dist) dist[i] = d;
         if (nrec != n - 1) atomicOr(status, 0x4u);
     }
+    if (mo.mark) {
+        __syncwarp();  // the lanes' slot writes ordered before the reads below
+        mark_net_slots(g, bv, mo, i, out, n, lane, 32, status);
+    }
 }
 
 constexpr int kMstWarpCosts = kMstWarpPins * (kMstWarpPins - 1) / 2;
 
 __global__ void __launch_bounds__(256) k_mst_warp(GridC g, BatchView bv, const float *__restrict__ cost,
                                                   int64_t *__restrict__ mst, float *__restrict__ dist,
-                                                  uint32_t *status) {
+                                                  uint32_t *status, MarkOut mo) {
     __shared__ unsigned long long skey[8][32];
     __shared__ int scomp[8][32];
     __shared__ float sw[8][kMstWarpCosts];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int t = blockIdx.x * (blockDim.x >> 5) + wib;
     if (t >= bv.nm) return;
-    mst_warp_net(bv, cost, mst, dist, status, bv.order[bv.n2 + t], skey[wib], scomp[wib], sw[wib], lane);
+    mst_warp_net(g, bv, mo, cost, mst, dist, status, bv.order[bv.n2 + t], skey[wib], scomp[wib], sw[wib], lane);
 }
 
 // ---------------------------------------------------------------- Boruvka, one persistent launch
@@ -1257,7 +1341,8 @@ constexpr size_t kQueueWarpSmem = (size_t)kQueueWarps * (32 * 8 + 32 * 4 + kMstW
 __global__ void __launch_bounds__(kQueueThreads) k_mst_queue(GridC g, BatchView bv, const float *__restrict__ cost,
                                                             int64_t *__restrict__ mst, float *__restrict__ dist,
                                                             uint32_t *status, uint32_t *__restrict__ gmat,
-                                                            int64_t gmat_stride, int *__restrict__ queue) {
+                                                            int64_t gmat_stride, int *__restrict__ queue,
+                                                            MarkOut mo) {
     extern __shared__ unsigned long long sm[];
     __shared__ int warp_sums[32];
     __shared__ int s_total, s_item;
@@ -1278,10 +1363,12 @@ __global__ void __launch_bounds__(kQueueThreads) k_mst_queue(GridC g, BatchView 
         if (item >= total) break;
         if (item < nlarge) {  // nets above 128 pins first, then 33..128
             const int t = item < nbig ? bv.nmid + item : item - nbig;
-            mst_block_net(bv, cost, mst, dist, status, a, M, bv.order[bv.n2 + bv.nm + t], warp_sums, &s_total);
+            mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, bv.order[bv.n2 + bv.nm + t], warp_sums,
+                          &s_total);
         } else {
             const int t = (item - nlarge) * kQueueWarps + warp;
-            if (t < bv.nm) mst_warp_net(bv, cost, mst, dist, status, bv.order[bv.n2 + t], skey, scomp, sw, lane);
+            if (t < bv.nm)
+                mst_warp_net(g, bv, mo, cost, mst, dist, status, bv.order[bv.n2 + t], skey, scomp, sw, lane);
             __syncthreads();
         }
     }
@@ -1296,209 +1383,29 @@ __global__ void __launch_bounds__(kQueueThreads) k_mst_queue(GridC g, BatchView 
 }
 
 // ---------------------------------------------------------------- commit
-// The GCELLs of one committed edge (mst_bit_commit.hpp:36-67, 209-231): a
-// layer change covers its interior layers, a wire its inclusive span. Each
-// cell is visited once: V::span(first id, count) for a wire (ids contiguous
-// along the track), V::cell(id) for a via cell. Only stacked pins (same x
-// and y) can revisit a cell -- the two layer changes and the one-cell wire
-// share a column -- so that case visits the union of their layers.
-__device__ __forceinline__ uint64_t layer_interior(int a, int b) {
-    const int lo = a < b ? a : b, hi = a < b ? b : a;
-    if (hi - lo < 2) return 0;
-    return ((1ull << hi) - 1) & ~((1ull << (lo + 1)) - 1);
-}
-
-template <class V>
-__device__ __forceinline__ bool walk_edge(const GridC &g, int z1, int x1, int y1, int z2, int x2, int y2, int cpat,
-                                          V &vis) {
-    const int via1 = cpat / g.Z2, v = cpat % g.Z2;
-    const bool bth = (x1 != x2 && y1 != y2);
-    const int via2 = (via1 & 1) ? 2 * v : 2 * v + 1;
-    if (cpat < 0 || via1 < 1 || via1 >= g.Z || (bth && via2 != 0 && via2 >= g.Z)) return false;
-    if (x1 == x2 && y1 == y2) {
-        uint64_t m = layer_interior(z1, via1) | (1ull << via1) | layer_interior(via1, z2);
-        while (m) {
-            const int i = __ffsll((long long)m) - 1;
-            m &= m - 1;
-            vis.cell(enc(g, i, x1, y1));
+// The marking of a caller's MST slots (the mst_bit_commit boundary, whose
+// trees were built elsewhere; the route marks inside the tree kernels): one
+// thread per slot of the batch -- its net from the slot offsets, the slot
+// checked to be an edge of that net (mst_bit_commit.hpp:81-105) and its path
+// marked.
+__global__ void __launch_bounds__(256) k_mark(GridC g, BatchView bv, const int64_t *__restrict__ mst, MarkOut mo,
+                                              uint32_t *status) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < bv.n_nodes;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        const int net = ofs_search(bv.node_ofs, bv.n, s);
+        const int64_t E = mst[s];
+        if (E == -1) {
+            if (mo.mst_pat) mo.mst_pat[s] = -1;
+            continue;
         }
-        return true;
-    }
-    auto via = [&](int za, int zb) {
-        const int lo = za < zb ? za : zb, hi = za < zb ? zb : za;
-        for (int i = lo + 1; i < hi; i++) vis.cell(enc(g, i, x1, y1));
-    };
-    auto wire = [&](int z) {
-        if (z & 1) {
-            const int lo = min(y1, y2), hi = max(y1, y2);
-            vis.span(z * g.XY + x1 * g.Y + lo, hi - lo + 1);
-            y1 = y2;
-        } else {
-            const int lo = min(x1, x2), hi = max(x1, x2);
-            vis.span(z * g.XY + y1 * g.X + lo, hi - lo + 1);
-            x1 = x2;
+        const int n = bv.npin[net];
+        const int u = (int)((E >> 15) & 0x7fff), v = (int)(E & 0x7fff);
+        if ((E >> 30) != net || u >= n || v >= n || u == v) {
+            atomicOr(status, 0x1u);
+            if (mo.mst_pat) mo.mst_pat[s] = -1;
+            continue;
         }
-    };
-    if (z1 != via1) {
-        via(z1, via1);
-        z1 = via1;
-    }
-    wire(z1);
-    if (bth && via2 != 0 && z1 != via2) {
-        via(z1, via2);
-        z1 = via2;
-        wire(z1);
-    }
-    if (z1 != z2) via(z1, z2);
-    return x1 == x2 && y1 == y2;
-}
-
-// decodes MST slot s of the batch; false for sentinels and invalid slots
-struct EdgeRef {
-    int net, cpat, z1, x1, y1, z2, x2, y2;
-};
-__device__ __forceinline__ int edge_of(const GridC &g, const BatchView &bv, const int32_t *__restrict__ pins,
-                                       const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                       int64_t s, int net, EdgeRef &r) {
-    r.net = net;
-    const int64_t E = mst[s];
-    if (E == -1) return 0;
-    const int n = bv.npin[r.net];
-    int n1 = (int)(E & 0x7fff), n2 = (int)((E >> 15) & 0x7fff);
-    if ((E >> 30) != r.net || n1 >= n || n2 >= n || n1 == n2) return -1;
-    if (n1 < n2) {
-        const int t = n1;
-        n1 = n2;
-        n2 = t;
-    }
-    r.cpat = ppat[bv.pair_ofs[r.net] + (int64_t)n1 * (n1 - 1) / 2 + n2];
-    const int32_t *np = pins + bv.pin_base[r.net];
-    dec(g, __ldg(np + n1), r.z1, r.x1, r.y1);
-    dec(g, __ldg(np + n2), r.z2, r.x2, r.y2);
-    return 1;
-}
-
-// The marking units of one edge's path: each via cell, and each 32-cell mark
-// word a wire covers (with the word's bits inside the wire).
-// A path has at most three layer changes of up to Z-2 interior cells and two
-// wires.
-constexpr int kPathSegs = 3 * kMaxLayers + 2;
-struct PathUnits {
-    int seg_n;                    // set to 0 before the walk
-    int seg_kind[kPathSegs];      // 0: via cell, 1: wire
-    int32_t seg_a[kPathSegs];     // via: cell id; wire: first cell id
-    int seg_b[kPathSegs];         // wire: cell count
-    int seg_u[kPathSegs + 1];     // prefix of unit counts
-    __device__ void cell(int32_t e) {
-        seg_kind[seg_n] = 0;
-        seg_a[seg_n] = e;
-        seg_b[seg_n] = 1;
-        seg_u[seg_n + 1] = seg_u[seg_n] + 1;
-        seg_n++;
-    }
-    __device__ void span(int32_t e0, int cnt) {
-        seg_kind[seg_n] = 1;
-        seg_a[seg_n] = e0;
-        seg_b[seg_n] = cnt;
-        seg_u[seg_n + 1] = seg_u[seg_n] + ((e0 + cnt - 1) >> 5) - (e0 >> 5) + 1;
-        seg_n++;
-    }
-    // word and mask of unit u
-    __device__ void unit(int u, int &w, uint32_t &m) const {
-        int s = 0;
-        while (seg_u[s + 1] <= u) s++;
-        const int k = u - seg_u[s];
-        if (seg_kind[s] == 0) {
-            w = seg_a[s] >> 5;
-            m = 1u << (seg_a[s] & 31);
-            return;
-        }
-        const int32_t e0 = seg_a[s], e1 = e0 + seg_b[s] - 1;
-        w = (e0 >> 5) + k;
-        m = 0xffffffffu;
-        if (w == (e0 >> 5)) m &= 0xffffffffu << (e0 & 31);
-        if (w == (e1 >> 5)) m &= 0xffffffffu >> (31 - (e1 & 31));
-    }
-};
-
-
-// ---------------------------------------------------------------- commit by track
-
-// track index and first cell of the track holding cell e
-__device__ __forceinline__ void track_of(const GridC &g, int32_t e, int &t, int32_t &base) {
-    const int z = e / g.XY;
-    const int r = e - z * g.XY;
-    const int L = (z & 1) ? g.Y : g.X;
-    const int row = r / L;
-    t = track_first(g, z) + row;
-    base = z * g.XY + row * L;
-}
-
-// One warp per MST slot (mst_bit_commit.hpp:147-235): the warp walks the
-// slot's L path and sets the mark bits of its GCELLs with atomicOr. What the
-// batch records is the set of tracks that gained marked cells: each path
-// unit (a via cell, or the part of a wire inside one 32-cell mark word) lies
-// in a single track, and the first unit to set bits of a track flags it in a
-// track bitmap and appends the track's first cell to the track list.
-// Slots k0..k1-1 of the batch are marked; with `sorder` they are entries
-// k0..k1-1 of the class-ordered slot list, so that each size class can be
-// marked on its own stream right after its trees are built (marking is
-// order-independent: bits are ORed, tracks listed as a set).
-__global__ void __launch_bounds__(256) k_mark7(GridC g, BatchView bv, const int32_t *__restrict__ pins,
-                                               const int64_t *__restrict__ mst, const int16_t *__restrict__ ppat,
-                                               int32_t *__restrict__ mst_pat, uint32_t *mark, uint32_t *tbits,
-                                               int32_t *__restrict__ tlist, int32_t *tcount, uint32_t *status,
-                                               const int32_t *__restrict__ sorder, int64_t k0, int64_t k1) {
-    __shared__ PathUnits su[8];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    PathUnits &pu = su[wib];
-    for (int64_t kk = k0 + (int64_t)blockIdx.x * (blockDim.x >> 5) + wib; kk < k1; kk += nwarps) {
-        const int64_t s = sorder ? (int64_t)__ldg(sorder + kk) : kk;
-        int units = 0;
-        const int net = bv.slot_net ? __ldg(bv.slot_net + s) : warp_ofs_search(bv.node_ofs, bv.n, s, lane);
-        if (lane == 0) {
-            pu.seg_n = 0;
-            pu.seg_u[0] = 0;
-            EdgeRef r;
-            const int ok = edge_of(g, bv, pins, mst, ppat, s, net, r);
-            if (ok <= 0) {
-                if (mst_pat) mst_pat[s] = -1;
-                if (ok < 0) atomicOr(status, 0x1u);
-            } else {
-                if (mst_pat) mst_pat[s] = r.cpat;
-                if (!walk_edge(g, r.z1, r.x1, r.y1, r.z2, r.x2, r.y2, r.cpat, pu)) atomicOr(status, 0x2u);
-            }
-            units = pu.seg_u[pu.seg_n];
-        }
-        units = __shfl_sync(FULL, units, 0);
-        __syncwarp();
-        for (int u0 = 0; u0 < units; u0 += 32) {
-            const int u = u0 + lane;
-            int32_t tb = 0;
-            bool fresh = false;
-            if (u < units) {
-                int w;
-                uint32_t m;
-                pu.unit(u, w, m);
-                const uint32_t old = atomicOr(mark + w, m);
-                if (m & ~old) {
-                    int t;
-                    track_of(g, (w << 5) + __ffs(m) - 1, t, tb);
-                    const uint32_t bit = 1u << (t & 31);
-                    fresh = !(atomicOr(tbits + (t >> 5), bit) & bit);
-                }
-            }
-            const unsigned want = __ballot_sync(FULL, fresh);
-            if (want) {
-                int base = 0;
-                if (lane == 0) base = atomicAdd(tcount, __popc(want));
-                base = __shfl_sync(FULL, base, 0);
-                if (fresh) tlist[base + __popc(want & ((1u << lane) - 1))] = tb;
-            }
-        }
-        __syncwarp();
+        mark_edge_slot(g, bv, mo, net, s, u, v, status);
     }
 }
 
@@ -1506,22 +1413,22 @@ constexpr int kTrackWarpsMax = 8;  // warps per k_track_commit block
 constexpr int kTrackWords = 48;    // mark words per track in the node sweep's rank table
 constexpr int kTrackSweepMin = 64; // tracks with more marked cells update by node
 
-// One warp per listed track (bit_util.hpp:75-90 for the cells the batch
-// marked on it): (1) the marked positions of the track and their increments
-// cost(cap-1) - cost(cap) are compacted in ascending order (shared memory
-// when the track fits, else the track's slice of a CSIZE scratch), each
-// cell's capacity drops by one and its mark bit is cleared; (2) every marked
-// cell walks its update path and, for each node where it is the highest
-// marked cell of the node's range (i - lowbit(i), i], adds the increments of
-// that range's marked cells to the node in ascending order -- the node's
-// updates in cell order, as a sequential commit makes them. Nodes thus have
-// one writer each; the track's cells are touched by this warp alone.
-__global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__restrict__ tlist,
-                                                      const int32_t *__restrict__ tcount, uint32_t *mark,
-                                                      uint32_t *tbits, int32_t *__restrict__ capr,
-                                                      const float *__restrict__ dlut, float *__restrict__ fen,
-                                                      int32_t *__restrict__ gpos, float *__restrict__ gdel,
-                                                      int cap, const float *__restrict__ pred, float beta) {
+// One warp per routing track, every track of the grid (bit_util.hpp:75-90
+// for the cells the batch marked on it; a track without marks costs one read
+// of its mark words): (1) the marked positions of the track and their
+// increments cost(cap-1) - cost(cap) are compacted in ascending order (shared
+// memory when the track fits, else the track's slice of a CSIZE scratch),
+// each cell's capacity drops by one and its mark bit is cleared; (2) every
+// marked cell walks its update path and, for each node where it is the
+// highest marked cell of the node's range (i - lowbit(i), i], adds the
+// increments of that range's marked cells to the node in ascending order --
+// the node's updates in cell order, as a sequential commit makes them. Nodes
+// thus have one writer each; the track's cells are touched by this warp alone.
+__global__ void __launch_bounds__(256) k_track_commit(GridC g, int n_tracks, uint32_t *mark,
+                                                      int32_t *__restrict__ capr, const float *__restrict__ dlut,
+                                                      float *__restrict__ fen, int32_t *__restrict__ gpos,
+                                                      float *__restrict__ gdel, int cap,
+                                                      const float *__restrict__ pred, float beta) {
     extern __shared__ int32_t tsm[];  // per warp: cap positions, then cap increments
     // per warp: the track's mark words and the marked cells before each word
     __shared__ uint32_t s_wm[kTrackWarpsMax][kTrackWords];
@@ -1530,13 +1437,13 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     uint32_t *wm = s_wm[wib];
     int *wk = s_wk[wib];
-    const int cnt = *tcount;
     int32_t *spos = tsm + (size_t)wib * 2 * cap;
     float *sdel = reinterpret_cast<float *>(spos + cap);
-    for (int t = blockIdx.x * wpb + wib; t < cnt; t += gridDim.x * wpb) {
-        const int32_t base = tlist[t];
-        const int z = base / g.XY;
+    for (int t = blockIdx.x * wpb + wib; t < n_tracks; t += gridDim.x * wpb) {
+        int z = 0;
+        while (z + 1 < g.Z && track_first(g, z + 1) <= t) z++;
         const int L = (z & 1) ? g.Y : g.X;
+        const int32_t base = z * g.XY + (t - track_first(g, z)) * L;
         const int w0 = base >> 5, w1 = (base + L - 1) >> 5;
         // marked count of the track
         int total = 0;
@@ -1547,6 +1454,7 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
             total += __popc(m);
         }
         total = __reduce_add_sync(FULL, total);
+        if (total == 0) continue;  // warp-uniform
         int32_t *P = total <= cap ? spos : gpos + base;
         float *D = total <= cap ? sdel : gdel + base;
         // heavily marked tracks update by node (the per-cell walks would
@@ -1677,36 +1585,46 @@ __global__ void __launch_bounds__(256) k_track_commit(GridC g, const int32_t *__
             if (k >= total) continue;
             const int p = P[k];
             const int nxt = k + 1 < total ? P[k + 1] : L;  // next marked position (L: none)
-            for (int i = p + 1; i <= L && nxt >= i; i += i & -i) {
-                float v = fen[base + i - 1];  // in flight during the search
-                const int lo = i - (i & -i);  // range [lo, i-1], 0-based
-                int a = 0, b = k;             // first index with P >= lo
-                while (a < b) {
-                    const int mid = (a + b) >> 1;
-                    if (P[mid] < lo) a = mid + 1;
-                    else b = mid;
-                }
-                // the range's increments in cell order, eight loads ahead of
-                // their additions
-                int j = a;
-                for (; j + 8 <= k + 1; j += 8) {
-                    float d[8];
+            // this cell's nodes are p+1, then + lowbit, ... while <= nxt (and
+            // so <= L); their values are loaded eight at a time before any
+            // is updated (no other lane writes them)
+            int i = p + 1;
+            while (i <= nxt) {
+                float v[8];
+                int node[8];
 #pragma unroll
-                    for (int u = 0; u < 8; u++) d[u] = D[j + u];
-#pragma unroll
-                    for (int u = 0; u < 8; u++) v += d[u];
+                for (int u = 0; u < 8; u++) {
+                    node[u] = i <= nxt ? i : 0;
+                    v[u] = node[u] ? fen[base + i - 1] : 0.0f;
+                    if (node[u]) i += i & -i;
                 }
-                for (; j <= k; j++) v += D[j];
-                fen[base + i - 1] = v;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    if (!node[u]) continue;
+                    const int lo = node[u] - (node[u] & -node[u]);  // range [lo, node-1], 0-based
+                    int a = 0, b = k;                               // first index with P >= lo
+                    while (a < b) {
+                        const int mid = (a + b) >> 1;
+                        if (P[mid] < lo) a = mid + 1;
+                        else b = mid;
+                    }
+                    // the range's increments in cell order, eight loads
+                    // ahead of their additions
+                    float x = v[u];
+                    int j = a;
+                    for (; j + 8 <= k + 1; j += 8) {
+                        float d[8];
+#pragma unroll
+                        for (int q = 0; q < 8; q++) d[q] = D[j + q];
+#pragma unroll
+                        for (int q = 0; q < 8; q++) x += d[q];
+                    }
+                    for (; j <= k; j++) x += D[j];
+                    fen[base + node[u] - 1] = x;
+                }
             }
         }
         __syncwarp();
-        if (lane == 0) {
-            int tt;
-            int32_t bb;
-            track_of(g, base, tt, bb);
-            atomicAnd(tbits + (tt >> 5), ~(1u << (tt & 31)));
-        }
     }
 }
 

@@ -40,6 +40,11 @@ class LookaheadNet:
 
     __del__ = close
 
+    def check(self) -> None:
+        """Waits for work enqueued by stream-ordered calls (a captured learned
+        route) and raises if a convolution gave up waiting for its results."""
+        check(self._lib.gr_cnn_check(self._h), "gr_cnn_check")
+
     @property
     def num_params(self) -> int:
         return int(self._lib.gr_cnn_num_params(self._h))

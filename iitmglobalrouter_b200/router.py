@@ -246,6 +246,17 @@ class Router:
                                                        ptr(mst_out), ptr(pat_out) if pat_out is not None else None),
               "gr_route_design_lookahead_host")
 
+    def route_lookahead_plan(self, net, every: int, beta: float, mode: str, mst, pat=None, graph=True,
+                             stream=None):
+        """The same learned route into device tensors laid out as route_plan's
+        (gr_route_plan_lookahead), as one captured CUDA graph when `graph`;
+        enqueued on the context's stream (or `stream`) without waiting."""
+        modes = {"demand": _capi.GR_LA_DEMAND, "excess": _capi.GR_LA_EXCESS}
+        self._after_torch(stream, mst, pat)
+        check(self._lib.gr_route_plan_lookahead(self._h, net._h, every, C.c_float(beta), modes[mode], ptr(mst),
+                                                ptr(pat), GR_PLAN_GRAPH if graph else 0, stream),
+              "gr_route_plan_lookahead")
+
     # ---------------------------------------------------------- lookahead
     def features(self, scale: float = 1.0 / 16):
         """Network input from the current state: (2Z, Y, X) CUDA float32."""

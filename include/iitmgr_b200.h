@@ -205,6 +205,16 @@ int gr_set_lookahead(gr_ctx *ctx, const float *d_pred, float beta, void *stream)
 typedef struct gr_cnn gr_cnn;
 int gr_route_design_lookahead_host(gr_ctx *ctx, gr_cnn *cnn, int32_t every, float beta, int mode,
                                    int64_t *h_mst_edges, int32_t *h_mst_pat);
+/* The same learned route into device buffers laid out as gr_route_plan's,
+ * on `stream`, without waiting for it: the features, the network's forward
+ * pass, the prediction transform, the Fenwick rebuilds and every batch are
+ * device work, so with GR_PLAN_GRAPH the whole route is one captured CUDA
+ * graph (kept and replayed while the plan, buffers, network and settings are
+ * unchanged). Ends with the plain cost restored; gr_sync and gr_cnn_check
+ * report device errors. (The host entry above calls this with
+ * GR_PLAN_GRAPH.) */
+int gr_route_plan_lookahead(gr_ctx *ctx, gr_cnn *cnn, int32_t every, float beta, int mode, int64_t *d_mst_edges,
+                            int32_t *d_mst_pat, int flags, void *stream);
 
 /* Launch shapes of the Boruvka size classes (results do not depend on them;
  * the autotuner in iitmglobalrouter_b200/tune.py picks them per GPU and Z). */
@@ -295,6 +305,13 @@ int gr_cnn_info(gr_cnn *cnn, int *device, int *in_channels, int *out_channels, i
 int gr_cnn_get_params(gr_cnn *cnn, float *h_out);
 int gr_cnn_set_params(gr_cnn *cnn, const float *h_in);
 int gr_cnn_forward(gr_cnn *cnn, const float *d_in, float *d_out);
+/* the same forward pass enqueued on `stream` (NULL: the network's own
+ * stream) without waiting for it, so that it can be captured in a CUDA graph
+ * with other work; gr_cnn_check later waits for the network's stream and
+ * reports a convolution that gave up waiting for its tensor-core results
+ * (GR_ERR_DEVICE). The network's buffers are shared by every call. */
+int gr_cnn_forward_async(gr_cnn *cnn, const float *d_in, float *d_out, void *stream);
+int gr_cnn_check(gr_cnn *cnn);
 /* loss and gradients (host, parameter layout) without an update */
 int gr_cnn_grads(gr_cnn *cnn, const float *d_in, const float *d_target, float *h_grads, float *h_loss);
 int gr_cnn_train_step(gr_cnn *cnn, const float *d_in, const float *d_target, float lr, float *h_loss);

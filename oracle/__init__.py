@@ -37,6 +37,7 @@ _SIG = {
     "gro_route_batch": (_I, [_P, _P, _P, _P, _I32, _P, _P, _P, _P, _P, _I]),
     "gro_route_batches": (_I, [_P, _P, _P, _P, _P, _I32, _P, _P, _I]),
     "gro_count_oob_pairs": (None, [_P, _P, _P, _P, _I32, _P]),
+    "gro_lpattern_top2": (None, [_P, _P, _I64, _P, _P, _P, _I]),
 }
 _lib = None
 
@@ -115,6 +116,22 @@ class Grid:
         pat = np.empty(n, dtype=np.int16)
         lib().gro_lpattern(self._h, _p(pairs), n, _p(cost), _p(pat), nthreads)
         return cost, pat
+
+    def lpattern_top2(self, pairs, nthreads=1):
+        """(cost, pattern, cheapest cost among the other valid patterns)."""
+        pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+        n = pairs.size // 2
+        cost = np.empty(n, dtype=np.float32)
+        pat = np.empty(n, dtype=np.int16)
+        cost2 = np.empty(n, dtype=np.float32)
+        lib().gro_lpattern_top2(self._h, _p(pairs), n, _p(cost), _p(pat), _p(cost2), nthreads)
+        return cost, pat, cost2
+
+    def set_state(self, capr, fen):
+        """Overwrites the remaining capacities and the Fenwick nodes (a cost
+        state recorded elsewhere, e.g. by the reference's own code)."""
+        np.ctypeslib.as_array(self._s.capr, shape=(self.csize,))[:] = np.asarray(capr, dtype=np.int32)
+        np.ctypeslib.as_array(self._s.fen, shape=(self.csize,))[:] = np.asarray(fen, dtype=np.float32)
 
     def commit(self, pin_ofs, pins, net_ids, mst, pair_pat):
         pin_ofs = np.ascontiguousarray(pin_ofs, dtype=np.int64)

@@ -212,6 +212,39 @@ void gro_lpattern_pair(const gro_grid *g, int32_t enc_src, int32_t enc_dst, floa
     *pat = (int16_t)bp;
 }
 
+/* The same argmin, with the cheapest cost among the pair's other valid
+ * patterns (+inf if none): a pair whose two values are equal is a tie, where
+ * the reference's kernel may store any of the tied patterns
+ * (bit_util.hpp:182-189). */
+void gro_lpattern_top2(const gro_grid *g, const int32_t *pairs, int64_t n_pairs, float *cost, int16_t *pat,
+                       float *cost2, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads > 0 ? nthreads : 1)
+    for (int64_t i = 0; i < n_pairs; i++) {
+        const int Z2 = (g->Z + 1) / 2, npat = g->Z * Z2;
+        float best = INFINITY, second = INFINITY;
+        int bp = -1, first = -1;
+        for (int cpat = 0; cpat < npat; cpat++) {
+            float c;
+            if (!gro_pattern_cost(g, pairs[2 * i], pairs[2 * i + 1], cpat, &c)) continue;
+            if (first < 0) first = cpat;
+            if (c < best) {
+                second = best;
+                best = c;
+                bp = cpat;
+            } else if (c < second) {
+                second = c;
+            }
+        }
+        if (bp < 0) {
+            bp = first;
+            best = INFINITY;
+        }
+        cost[i] = best;
+        pat[i] = (int16_t)bp;
+        cost2[i] = second;
+    }
+}
+
 void gro_lpattern(const gro_grid *g, const int32_t *pairs, int64_t n_pairs, float *cost, int16_t *pat,
                   int nthreads) {
     (void)nthreads;
@@ -395,13 +428,14 @@ typedef struct {
     int64_t nlist;
 } mark_ctx;
 
-static void mark_cell(mark_ctx *m, int z, int x, int y) {
-    int32_t e = gro_enc(m->g, z, x, y);
+static void mark_id(mark_ctx *m, int32_t e) {
     if (!m->mark[e]) {
         m->mark[e] = 1;
         m->list[m->nlist++] = e;
     }
 }
+
+static void mark_cell(mark_ctx *m, int z, int x, int y) { mark_id(m, gro_enc(m->g, z, x, y)); }
 
 /* mst_bit_commit.hpp:36-67 gpu_hash_gcell: a layer change marks the
  * interior layers only; a wire marks every cell of its inclusive span */
@@ -476,11 +510,25 @@ int gro_commit(gro_grid *g, const int64_t *pin_ofs, const int32_t *pins, const i
                 continue;
             }
             /* mst_bit_commit.hpp:209-231 */
+            int d = 0; /* interior cells of the first layer change */
             if (z1 != via1) {
                 walk_via(&m, z1, via1, x1, y1);
+                d = (z1 < via1 ? via1 - z1 : z1 - via1) - 1;
                 z1 = via1;
             }
-            if (z1) walk_wire(&m, z1, &x1, &y1, x2, y2);
+            if (z1) {
+                /* The first wire's cell ids are contiguous from `first`. In
+                 * gpu_commit_edge the threads of the first layer change's d
+                 * interior cells reach this wire with a negative local index
+                 * (-d .. -1), and this one call is not guarded by tid >= 0
+                 * (mst_bit_commit.hpp:216, unlike :213, :223-225, :228), so
+                 * gpu_hash_gcell (:49-66) also marks the d cells just below
+                 * the wire's lower end: cell ids first-d .. first-1, wrapping
+                 * into the previous track when that end is at coordinate 0. */
+                int32_t first = (z1 & 1) ? gro_enc(g, z1, x1, y1 < y2 ? y1 : y2) : gro_enc(g, z1, x1 < x2 ? x1 : x2, y1);
+                for (int k = 1; k <= d; k++) mark_id(&m, first - k);
+                walk_wire(&m, z1, &x1, &y1, x2, y2);
+            }
             if (bth_diff && via2 != 0) {
                 if (z1 != via2) {
                     walk_via(&m, z1, via2, x1, y1);

@@ -71,6 +71,10 @@ void gro_lpattern_pair(const gro_grid *g, int32_t enc_src, int32_t enc_dst, floa
 void gro_lpattern(const gro_grid *g, const int32_t *pairs, int64_t n_pairs,
                   float *cost, int16_t *pat, int nthreads);
 
+/* the argmin plus the cheapest cost among each pair's other valid patterns */
+void gro_lpattern_top2(const gro_grid *g, const int32_t *pairs, int64_t n_pairs,
+                       float *cost, int16_t *pat, float *cost2, int nthreads);
+
 /* pair list of a batch in reference order, test_lpat.hpp:313-333 */
 int64_t gro_batch_pairs(const int64_t *pin_ofs, const int32_t *pins,
                         const int32_t *net_ids, int32_t n_nets, int32_t *pairs);

@@ -79,15 +79,20 @@ def boruvka_kat():
 def commit_kat():
     # mst_bit_commit.hpp:36-67,209-231: walk from the higher pin index (src)
     # to the lower; a via marks its interior layers only, a wire marks its
-    # inclusive span. Cells as [z, x, y].
+    # inclusive span. The first wire is walked (:216) also by the threads of
+    # the first via's d interior cells, with local index -d..-1: they mark
+    # the d cells below the wire's lower end. Cells as [z, x, y].
     cases = [
-        # (0,5,2)->(0,1,2), pattern 4 = via1 2: via 0->2 marks layer 1, wire
-        # x = 1..5 on layer 2, via 2->0 marks layer 1
+        # (0,5,2)->(0,1,2), pattern 4 = via1 2: via 0->2 marks layer 1 (d = 1),
+        # wire x = 1..5 on layer 2 and the cell x = 0 below it, via 2->0 marks
+        # layer 1
         dict(name="x_only", grid=[8, 8, 4], src=[0, 5, 2], dst=[0, 1, 2], pattern=4,
-             cells=[[1, 5, 2], [2, 1, 2], [2, 2, 2], [2, 3, 2], [2, 4, 2], [2, 5, 2], [1, 1, 2]]),
-        # (3,2,2)->(0,2,2), pattern 2 = via1 1: via 3->1 marks layer 2, the
-        # zero-length wire still marks its one cell on layer 1
-        dict(name="stacked", grid=[8, 8, 4], src=[3, 2, 2], dst=[0, 2, 2], pattern=2, cells=[[2, 2, 2], [1, 2, 2]]),
+             cells=[[1, 5, 2], [2, 0, 2], [2, 1, 2], [2, 2, 2], [2, 3, 2], [2, 4, 2], [2, 5, 2], [1, 1, 2]]),
+        # (3,2,2)->(0,2,2), pattern 2 = via1 1: via 3->1 marks layer 2 (d = 1),
+        # the zero-length wire still marks its one cell on layer 1 and the
+        # cell y = 1 below it (layer 1 runs along y)
+        dict(name="stacked", grid=[8, 8, 4], src=[3, 2, 2], dst=[0, 2, 2], pattern=2,
+             cells=[[2, 2, 2], [1, 2, 1], [1, 2, 2]]),
         # (0,4,5)->(0,1,1), pattern 3 = via1 1, v 1 -> via2 2: wire y = 1..5 on
         # layer 1 at x 4, wire x = 1..4 on layer 2 at y 1, via 2->0 marks 1
         dict(name="bend", grid=[8, 8, 4], src=[0, 4, 5], dst=[0, 1, 1], pattern=3,

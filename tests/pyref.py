@@ -161,9 +161,17 @@ class PyGrid:
             return x2, y
 
         bth = x1 != x2 and y1 != y2
+        d = 0
         if z1 != via1:
             via(z1, via1, x1, y1)
+            d = abs(z1 - via1) - 1
             z1 = via1
+        # mst_bit_commit.hpp:216 calls gpu_hash_gcell for the first wire even
+        # for the threads of the first layer change's d interior cells, whose
+        # local index is then -d..-1: they mark the d cells before the wire's
+        # lower end (contiguous cell ids, into the previous track at 0)
+        first = self.enc(z1, x1, min(y1, y2)) if z1 & 1 else self.enc(z1, min(x1, x2), y1)
+        cells.extend(first - k for k in range(1, d + 1))
         x1, y1 = wire(z1, x1, y1)
         via2 = 2 * v if z1 & 1 else 2 * v + 1
         if bth and via2 != 0 and z1 != via2:

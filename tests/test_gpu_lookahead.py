@@ -226,3 +226,32 @@ def test_route_cli_lookahead_matches_python_driver(cuda, tmp_path, mode):
     assert r.returncode == 0, r.stderr
     assert f"lookahead {mode}" in r.stdout
     assert out.read_bytes() == ref.read_bytes()
+
+
+def test_lookahead_plan_graph_replays_and_restores_plain_cost(cuda):
+    """gr_route_plan_lookahead as one captured graph (network forward passes,
+    prediction transforms, Fenwick rebuilds and every batch), captured once
+    and replayed: each run equals the stream-ordered run without a graph, and
+    afterwards the plain cost is back (a plain route gives the oracle's
+    result)."""
+    import torch
+
+    d, R, mst, pat, ofs, pins, bofs, ids = _setup(1, seed=3)
+    net = _strong_net(R, R.Z)
+    R.route_lookahead_plan(net, 4, 1.0, "excess", mst, pat, graph=False)
+    R.sync()
+    want = (mst.cpu().numpy(), pat.cpu().numpy(), R.demand())
+    for _ in range(2):
+        mst.fill_(-5)
+        torch.cuda.synchronize()
+        R.route_lookahead_plan(net, 4, 1.0, "excess", mst, pat, graph=True)
+        R.sync()
+        assert np.array_equal(mst.cpu().numpy(), want[0]) and np.array_equal(pat.cpu().numpy(), want[1])
+        assert np.array_equal(R.demand(), want[2])
+        R.reset()
+        R.route_plan(mst, pat, graph=True)
+        R.sync()
+        g = oracle.Grid(R.X, R.Y, R.Z, d.caps())
+        rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=8)
+        assert rc == 0 and np.array_equal(mst.cpu().numpy(), mst_c) and np.array_equal(pat.cpu().numpy(), mp_c)
+    assert R.status() == 0
