@@ -72,6 +72,49 @@ __device__ __forceinline__ float fen_query(const float *__restrict__ fen, int32_
     return res;
 }
 
+// The two prefix queries of one cell's point cost, Q(pos) and Q(pos - 1),
+// each summed exactly as fen_query sums it, with their shared nodes loaded
+// once. With i = pos + 1 and p = i with its lowest set bit cleared, Q(pos)
+// adds node i, then the nodes of p's path; Q(pos - 1) adds the nodes from
+// i - 1 down to (not including) p, then the same nodes of p's path.
+__device__ __forceinline__ float2 fen_query_pair(const float *__restrict__ fen, int32_t base, int pos) {
+    const int i = pos + 1, pre = i & (i - 1);
+    float r1 = 0.0f, r2 = 0.0f;
+    r1 += __ldg(fen + base + i - 1);
+    int k = i - 1;
+    while (k > pre) {
+        float v[8];
+        bool on[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            on[t] = k > pre;
+            v[t] = on[t] ? __ldg(fen + base + k - 1) : 0.0f;
+            if (on[t]) k &= k - 1;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; t++)
+            if (on[t]) r2 += v[t];
+    }
+    k = pre;
+    while (k > 0) {
+        float v[8];
+        bool on[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            on[t] = k > 0;
+            v[t] = on[t] ? __ldg(fen + base + k - 1) : 0.0f;
+            k &= k - 1;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; t++)
+            if (on[t]) {
+                r1 += v[t];
+                r2 += v[t];
+            }
+    }
+    return make_float2(r1, r2);
+}
+
 // Order-preserving 64-bit key of (cost, pair id): the Boruvka minimum is
 // the smallest cost, ties broken by the lowest pair id.
 // order-preserving bits of a cost: a < b as floats iff bits(a) < bits(b)
@@ -209,11 +252,8 @@ struct DirectEv {
     bool bth;
     __device__ State start() const { return State{x1, y1}; }
     __device__ float point(int z, int x, int y) const {
-        int32_t b = track_base(g, z, x, y);
-        int p = (z & 1) ? y : x;
-        float hi = fen_query(fen, b, p);
-        float lo = fen_query(fen, b, p - 1);
-        return hi - lo;
+        const float2 q = fen_query_pair(fen, track_base(g, z, x, y), (z & 1) ? y : x);
+        return q.x - q.y;
     }
     __device__ void via(int za, int zb, State s, float &c) const {
         int zmin = za < zb ? za : zb, zmax = za < zb ? zb : za;

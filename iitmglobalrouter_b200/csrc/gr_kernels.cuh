@@ -567,11 +567,7 @@ __global__ void k_qtable(GridC g, BatchView bv, Coords cd, const float *__restri
         const int64_t pb = bv.pin_base[net];
         const int x = __ldg(cd.cx + pb + a), y = __ldg(cd.cy + pb + b);
         const int32_t base = track_base(g, z, x, y);
-        const int pos = (z & 1) ? y : x;
-        float2 q;
-        q.x = fen_query(fen, base, pos);
-        q.y = fen_query(fen, base, pos - 1);
-        tab[t] = q;
+        tab[t] = fen_query_pair(fen, base, (z & 1) ? y : x);
     }
 }
 
@@ -1000,17 +996,22 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
 // Patterns of the first-via layers via1 with (via1 - 1) % S == SUB (all of
 // them for S = 1): the lowest-cost valid pattern (best, bp; bp = -1 when no
 // valid pattern has a finite cost) and the lowest valid pattern id (first).
-template <int ZC, int S, int SUB>
-__device__ __forceinline__ void lpat_regs_part(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
-                                               int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p,
+// Z1F / Z2F >= 0 fix the source / target layer at compile time (the caller
+// guarantees z1 == Z1F, z2 == Z2F): every via's layer range is then known to
+// the compiler and no addition is predicated on the pins' layers. BTHF >= 0
+// fixes whether the pins differ in both x and y (1) or not (0).
+template <int ZC, int S, int SUB, int Z1F = -1, int Z2F = -1, int BTHF = -1>
+__device__ __forceinline__ void lpat_regs_part(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1_,
+                                               int z2_, int xj, int yj, int xk, int yk, float &out_c, int &out_p,
                                                int &out_first) {
     constexpr int Z2 = (ZC + 1) / 2;
+    const int z1 = Z1F >= 0 ? Z1F : z1_, z2 = Z2F >= 0 ? Z2F : z2_;
     float Pj[ZC], Pk[ZC], Pc1[ZC], Pc2[ZC], W1[ZC], W2[ZC];
     const int64_t nn = (int64_t)nx * ny;
     const int xij = pj >> 16, yij = pj & 0xffff, xik = pk >> 16, yik = pk & 0xffff;
     const int ojj = xij * ny + yij, okk = xik * ny + yik, okj = xik * ny + yij, ojk = xij * ny + yik;
     const bool xlt = xj < xk, ylt = yj < yk;
-    const bool mx = xj != xk, my = yj != yk;
+    const bool mx = BTHF == 1 ? true : xj != xk, my = BTHF == 1 ? true : yj != yk;
 #pragma unroll
     for (int z = 0; z < ZC; z++) {
         const float2 *Tz = T + z * nn;
@@ -1027,7 +1028,7 @@ __device__ __forceinline__ void lpat_regs_part(const float2 *__restrict__ T, int
             W2[z] = xlt ? tkk.x - tjk.y : tjk.x - tkk.y;  // row y_k from C2
         }
     }
-    const bool bth = mx && my;
+    const bool bth = BTHF >= 0 ? BTHF == 1 : (mx && my);
     float best = __int_as_float(0x7f800000);
     int bp = -1, first = -1;
 #pragma unroll
@@ -1084,50 +1085,137 @@ __device__ __forceinline__ void lpat_regs_part(const float2 *__restrict__ T, int
 
 // all patterns of the pair: the cheapest, ties to the lowest id; with no
 // finite-cost valid pattern, the lowest valid id at cost +inf
-template <int ZC>
+template <int ZC, int Z1F = -1, int Z2F = -1, int BTHF = -1>
 __device__ __forceinline__ void lpat_regs(const float2 *__restrict__ T, int nx, int ny, int pj, int pk, int z1,
                                           int z2, int xj, int yj, int xk, int yk, float &out_c, int &out_p) {
     int first;
-    lpat_regs_part<ZC, 1, 0>(T, nx, ny, pj, pk, z1, z2, xj, yj, xk, yk, out_c, out_p, first);
+    lpat_regs_part<ZC, 1, 0, Z1F, Z2F, BTHF>(T, nx, ny, pj, pk, z1, z2, xj, yj, xk, yk, out_c, out_p, first);
     if (out_p < 0) {
         out_p = first;
         out_c = __int_as_float(0x7f800000);
     }
 }
 
+// Class of a pair: pins are ascending by cell id within a net, so the source
+// (the higher pin) has z1 >= z2. Pairs with both pins on layers 0-1 (where
+// pins usually sit) fall in layer classes 0 = (0, 0), 1 = (1, 0), 2 = (1, 1);
+// those whose pins differ in both x and y keep it, the others add 3. Class 6
+// is every other pair, the pairs of nets without a query table, and every
+// pair when Z is not 9 or 10 (the layer counts whose pattern bodies are
+// compiled per class).
+constexpr int kLpatClasses = 7;
+constexpr int kLpatBlock = 256;
+
 template <int ZC>
-__global__ void __launch_bounds__(256, 3) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins, Coords cd,
-                                                const float *__restrict__ fen, const float2 *__restrict__ tab,
-                                                float *__restrict__ cost, int16_t *__restrict__ pat,
-                                                int64_t *__restrict__ mst, float *__restrict__ dist, MarkOut mo,
-                                                uint32_t *status) {
-    const int lane = threadIdx.x & 31;
-    for (int64_t p0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); p0 < bv.n_pairs;
-         p0 += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t p = p0 + lane;
-        const int net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
-                                        p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
-        if (p >= bv.n_pairs) continue;
-        int j, k;
-        pair_decode(p - bv.pair_ofs[net], j, k);
-        const int32_t *np = pins + bv.pin_base[net];
-        int z1, x1, y1, z2, x2, y2;
-        dec(g, __ldg(np + j), z1, x1, y1);
-        dec(g, __ldg(np + k), z2, x2, y2);
-        float c;
-        int cp;
-        const int nxy = bv.nxy[net];
-        if (nxy) {
-            const int64_t pb = bv.pin_base[net];
-            lpat_regs<ZC>(tab + bv.tab_ofs[net], nxy >> 16, nxy & 0xffff, __ldg(cd.pxy + pb + j),
-                          __ldg(cd.pxy + pb + k), z1, z2, x1, y1, x2, y2, c, cp);
-        } else {
-            DirectEv ev{fen, g, z1, x1, y1, z2, x2, y2, (x1 != x2 && y1 != y2)};
-            lpat_argmin(ev, g, c, cp);
+__device__ __forceinline__ int lpat_class(bool table, int z1, int z2, bool bth) {
+    if (!table || (ZC != 9 && ZC != 10)) return 6;
+    int l = 3;
+    if (z2 == 0 && (z1 == 0 || z1 == 1)) l = z1;
+    else if (z1 == 1 && z2 == 1) l = 2;
+    return l == 3 ? 6 : l + (bth ? 0 : 3);
+}
+
+template <int ZC>
+__global__ void __launch_bounds__(kLpatBlock, 3) k_lpat_z(GridC g, BatchView bv, const int32_t *__restrict__ pins,
+                                                       Coords cd, const float *__restrict__ fen,
+                                                       const float2 *__restrict__ tab, float *__restrict__ cost,
+                                                       int16_t *__restrict__ pat, int64_t *__restrict__ mst,
+                                                       float *__restrict__ dist, MarkOut mo, uint32_t *status) {
+    // Per step a block takes 256 consecutive pairs: each thread decodes one
+    // (net by a warp search, pins, layer class), the block regroups them by
+    // class in shared memory, and each thread then evaluates the pair at its
+    // place in that order -- so a warp mostly holds pairs of one class and
+    // runs the pattern body compiled for that class's layers.
+    __shared__ int s_wcnt[kLpatBlock / 32][kLpatClasses];  // per warp and class: count, then first place
+    __shared__ int32_t s_off[kLpatBlock];                   // place -> pair offset in the step
+    __shared__ int32_t s_net[kLpatBlock], s_jk[kLpatBlock];
+    __shared__ uint32_t s_xy1[kLpatBlock], s_xy2[kLpatBlock];
+    __shared__ int16_t s_zz[kLpatBlock];
+    __shared__ int s_valid;
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t base = blockIdx.x * (int64_t)kLpatBlock; base < bv.n_pairs;
+         base += (int64_t)gridDim.x * kLpatBlock) {
+        const int64_t p0 = base + warp * 32, p = p0 + lane;
+        int cls = -1, net = 0, j = 0, k = 0, z1 = 0, x1 = 0, y1 = 0, z2 = 0, x2 = 0, y2 = 0;
+        if (p0 < bv.n_pairs) {  // warp-uniform
+            net = warp_ofs_window(bv.pair_ofs, bv.n, warp_ofs_search(bv.pair_ofs, bv.n, p0, lane),
+                                  p < bv.n_pairs ? p : bv.n_pairs - 1, lane);
+            if (p < bv.n_pairs) {
+                pair_decode(p - bv.pair_ofs[net], j, k);
+                const int32_t *np = pins + bv.pin_base[net];
+                dec(g, __ldg(np + j), z1, x1, y1);
+                dec(g, __ldg(np + k), z2, x2, y2);
+                cls = lpat_class<ZC>(bv.nxy[net] != 0, z1, z2, x1 != x2 && y1 != y2);
+            }
         }
-        cost[p] = c;
-        pat[p] = (int16_t)cp;
-        pin2_tree(g, bv, mo, net, c, cp, z1, x1, y1, z2, x2, y2, mst, dist, status);
+        unsigned m[kLpatClasses];
+#pragma unroll
+        for (int q = 0; q < kLpatClasses; q++) {
+            m[q] = __ballot_sync(FULL, cls == q);
+            if (lane == 0) s_wcnt[warp][q] = __popc(m[q]);
+        }
+        __syncthreads();
+        if (tid == 0) {  // places: class by class, warps in order within a class
+            int run = 0;
+#pragma unroll
+            for (int q = 0; q < kLpatClasses; q++)
+                for (int w = 0; w < kLpatBlock / 32; w++) {
+                    const int c = s_wcnt[w][q];
+                    s_wcnt[w][q] = run;
+                    run += c;
+                }
+            s_valid = run;
+        }
+        __syncthreads();
+        if (cls >= 0) {
+            const int at = s_wcnt[warp][cls] + __popc(m[cls] & ((1u << lane) - 1u));
+            s_off[at] = warp * 32 + lane;
+            s_net[at] = net;
+            s_jk[at] = (j << 16) | k;
+            s_xy1[at] = ((uint32_t)x1 << 16) | (uint32_t)y1;
+            s_xy2[at] = ((uint32_t)x2 << 16) | (uint32_t)y2;
+            s_zz[at] = (int16_t)((z1 << 8) | z2);
+        }
+        __syncthreads();
+        if (tid < s_valid) {
+            const int64_t q = base + s_off[tid];
+            const int n = s_net[tid], jk = s_jk[tid], zz = s_zz[tid];
+            const uint32_t a = s_xy1[tid], b = s_xy2[tid];
+            const int jj = jk >> 16, kk = jk & 0xffff;
+            const int za = zz >> 8, zb = zz & 0xff;
+            const int xa = (int)(a >> 16), ya = (int)(a & 0xffff), xb = (int)(b >> 16), yb = (int)(b & 0xffff);
+            const int nxy = bv.nxy[n];
+            const int c3 = lpat_class<ZC>(nxy != 0, za, zb, xa != xb && ya != yb);
+            float c;
+            int cp;
+            if (!nxy) {
+                DirectEv ev{fen, g, za, xa, ya, zb, xb, yb, (xa != xb && ya != yb)};
+                lpat_argmin(ev, g, c, cp);
+            } else {
+                const int64_t pb = bv.pin_base[n];
+                const float2 *T = tab + bv.tab_ofs[n];
+                const int pj = __ldg(cd.pxy + pb + jj), pk = __ldg(cd.pxy + pb + kk);
+                const int nx = nxy >> 16, ny = nxy & 0xffff;
+                if constexpr (ZC == 9 || ZC == 10) {
+                    switch (c3) {
+                        case 0: lpat_regs<ZC, 0, 0, 1>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        case 1: lpat_regs<ZC, 1, 0, 1>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        case 2: lpat_regs<ZC, 1, 1, 1>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        case 3: lpat_regs<ZC, 0, 0, 0>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        case 4: lpat_regs<ZC, 1, 0, 0>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        case 5: lpat_regs<ZC, 1, 1, 0>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp); break;
+                        default: lpat_regs<ZC>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp);
+                    }
+                } else {
+                    lpat_regs<ZC>(T, nx, ny, pj, pk, za, zb, xa, ya, xb, yb, c, cp);
+                }
+            }
+            cost[q] = c;
+            pat[q] = (int16_t)cp;
+            pin2_tree(g, bv, mo, n, c, cp, za, xa, ya, zb, xb, yb, mst, dist, status);
+        }
+        __syncthreads();  // the shared arrays are refilled by the next step
     }
 }
 
