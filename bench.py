@@ -17,6 +17,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -205,10 +206,11 @@ def make_workload(config, seed):
 
 def cpu_sample(ofs, pins, bofs, ids, target_pairs):
     """Strided batches of the plan whose pairs add up to about target_pairs."""
-    import iitmglobalrouter_b200 as gr
-
+    n = np.diff(np.asarray(ofs, np.int64))[np.asarray(ids)]
+    per_net = n * (n - 1) // 2
+    csum = np.concatenate([[0], np.cumsum(per_net)])
+    pairs = csum[np.asarray(bofs[1:], np.int64)] - csum[np.asarray(bofs[:-1], np.int64)]
     nb = len(bofs) - 1
-    pairs = np.array([gr.pair_count(ofs, ids[bofs[b]:bofs[b + 1]]) for b in range(nb)])
     stride = max(1, int(np.ceil(pairs.sum() / max(target_pairs, 1))))
     sel = list(range(0, nb, stride))
     sofs = [0]
@@ -219,14 +221,13 @@ def cpu_sample(ofs, pins, bofs, ids, target_pairs):
     return np.array(sofs, np.int64), np.concatenate(sids).astype(np.int32), stride, len(sel)
 
 
-def time_oracle(d, ofs, pins, sofs, sids, nthreads, keep=False):
+def time_oracle(dims, caps, ofs, pins, sofs, sids, nthreads, keep=False):
     """The oracle routes the sample's batches in order from the initial cost
     state (its Fenwick build inside the timed region, as the GPU step's
     reset is); with keep, also returns its grid and results."""
     import oracle
 
-    dims = d.dims
-    g = oracle.Grid(dims["X"], dims["Y"], dims["Z"], d.caps())
+    g = oracle.Grid(dims["X"], dims["Y"], dims["Z"], caps)
     t0 = time.perf_counter()
     g.reset()
     rc, mst, pat = g.route_batches(ofs, pins, sofs, sids, nthreads=nthreads)
@@ -260,29 +261,109 @@ def sample_parity(R, sofs, sids, ref):
     return f"bit-exact on {len(sids)} nets ({len(sofs) - 1} batches, {M} MST slots, all GCELLs and Fenwick nodes)"
 
 
+WRITE_DESIGN = """
+import sys, json, numpy as np
+sys.path.insert(0, sys.argv[1])
+import iitmglobalrouter_b200 as gr
+d = gr.Design.generate(int(sys.argv[2]), seed=int(sys.argv[3]))
+d.write(sys.argv[4] + "/design.cap", sys.argv[4] + "/design.net")
+ofs, pins = d.nets()
+bofs, ids = d.batch(4)
+np.savez(sys.argv[4] + "/plan.npz", caps=d.caps(), ofs=ofs, pins=pins, bofs=bofs, ids=ids)
+json.dump(d.dims, open(sys.argv[4] + "/dims.json", "w"))
+"""
+
+
+def reference_inputs(args, work):
+    """The untimed step before the reference arm, in a process of its own:
+    the design as .cap/.net text (and this library's plan of it, used only
+    when the reference's own reader and batcher cannot run here). The arm's
+    own process then loads nothing of this library."""
+    subprocess.run([sys.executable, "-c", WRITE_DESIGN, str(ROOT), str(args.config), str(args.seed), work],
+                   check=True, timeout=1800)
+    pl = np.load(Path(work) / "plan.npz")
+    dims = json.loads((Path(work) / "dims.json").read_text())
+    return dims, {k: pl[k] for k in pl.files}
+
+
+def reference_run(args, work, dims):
+    """The reference's own code path on the design (oracle/_ref/ref_harness,
+    built from its sources): its reader and batcher, then its per-batch
+    -bit_pmodel route (pair build, get_gpu_lpat_dist<5>, get_mst_tree<0> with
+    the commit) warmup + steps times from the initial cost state. Its kernels
+    exist for Z = 9 and 10 only; at other Z only the reader and batcher run.
+    Returns (plan arrays or None, per-pass route seconds or None, note)."""
+    harness = ROOT / "oracle" / "_ref" / "ref_harness"
+    if not harness.exists():
+        return None, None, "oracle/_ref/ref_harness not built (the reference's sources were absent at build time)"
+    out = Path(work) / "ref"
+    route = dims["Z"] in (9, 10)
+    cmd = [str(harness), "-cap", f"{work}/design.cap", "-net", f"{work}/design.net", "-out", str(out), "-new_fmt",
+           "-num_xdim_parts", "4", "-time_only", "-dump_plan", "-mst_cpu_threads", str(os.cpu_count() or 8)]
+    cmd += ["-repeat", str(args.warmup + args.steps)] if route else ["-no_route"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=3000)
+    if r.returncode != 0:
+        tail = (r.stderr.strip().splitlines() or ["no message"])[-1]
+        return None, None, f"ref_harness exited {r.returncode}: {tail[:200]}"
+    summ = json.loads((out / "summary.json").read_text())
+    rd = lambda name, dt: np.fromfile(out / name, dtype=dt)  # noqa: E731
+    bofs = rd("npart_ofst.i32", np.int32).astype(np.int64)
+    plan = {"caps": rd("caps.f32", np.float32).astype(np.int32), "ofs": rd("net_ofs.i64", np.int64),
+            "pins": rd("net_pins.i32", np.int32), "ids": rd("npart_ids.i32", np.int32),
+            "bofs": np.append(bofs, bofs[-1] + rd("npart_len.i32", np.int32)[-1])}
+    passes = summ.get("pass_route_s") if route else None
+    return plan, passes, f"reference reader {summ['read_s']:.1f} s, batcher {summ['batch_s']:.1f} s"
+
+
 def run_reference(args, rank):
-    """The reference arm: the reference's algorithm on the host cores (the
-    CPU oracle -- the reference's own GPU binary cannot be built here and its
-    sq_router CPU path does not compile)."""
+    """The reference arm. When the reference's own code was built here
+    (oracle/_ref/ref_harness) and its kernels exist for the design's Z, the
+    line times the reference's own per-batch route on this machine's GPU
+    (kind "reference"); otherwise the CPU oracle port routes a strided
+    sample of the plan with every host thread (kind "port"). Either way the
+    design comes from an untimed step in another process, and the plan is
+    the reference's own batches whenever its reader and batcher ran."""
     if rank != 0:
         return
-    d, ofs, pins, bofs, ids = make_workload(args.config, args.seed)
+    work = tempfile.mkdtemp(prefix="gr_ref_")
+    try:
+        dims, plan = reference_inputs(args, work)
+        ref_plan, passes, note = reference_run(args, work, dims)
+        plan_src = "the reference's reader and batcher" if ref_plan is not None else "this library's batcher"
+        if ref_plan is not None:
+            plan = ref_plan
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    ofs, pins, bofs, ids = plan["ofs"], plan["pins"], plan["bofs"], plan["ids"]
     nthreads = os.cpu_count() or 1
-    sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
-    for _ in range(args.warmup):
-        time_oracle(d, ofs, pins, sofs, sids, nthreads)
-    times = []
-    for _ in range(args.steps):
-        times.append(time_oracle(d, ofs, pins, sofs, sids, nthreads)[1])
-    t = sum(times) / len(times)
-    v = len(sids) / t
-    sample = f"every {stride}th batch of the plan ({nsel} batches, {len(sids)} nets) routed in order"
+    if passes:
+        timed = passes[args.warmup:] or passes
+        t = sum(timed) / len(timed)
+        n = len(ids)
+        v = n / t
+        sample = (f"every batch ({len(bofs) - 1} batches, {n} nets), the reference's -bit_pmodel route on cuda:0 "
+                  f"(pair build, get_gpu_lpat_dist<5>, get_mst_tree<0> with its commit), {len(passes)} passes "
+                  f"from the initial cost state, the last {len(timed)} timed; plan from {plan_src}; {note}")
+        base = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference", "sample": sample}
+    else:
+        sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
+        caps = plan["caps"]
+        for _ in range(args.warmup):
+            time_oracle(dims, caps, ofs, pins, sofs, sids, nthreads)
+        times = [time_oracle(dims, caps, ofs, pins, sofs, sids, nthreads)[1] for _ in range(args.steps)]
+        t = sum(times) / len(times)
+        v = len(sids) / t
+        sample = (f"one batch in {stride} of the plan ({nsel} batches, {len(sids)} nets) routed in order by the "
+                  f"oracle port; plan from {plan_src}; reference route not run: {note}")
+        base = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample}
+    maps = Path("/proc/self/maps")
+    loaded = maps.exists() and "libiitmgr_b200" in maps.read_text()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "seed": args.seed, "sample": sample},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "cpu_baseline": base, "product_library_loaded": loaded,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -455,9 +536,9 @@ def main():
     if rank == 0:
         sofs, sids, stride, nsel = cpu_sample(ofs, pins, bofs, ids, args.cpu_pairs)
         nthreads = os.cpu_count() or 1
-        v_cpu, dt, ref = time_oracle(d, ofs, pins, sofs, sids, nthreads, keep=True)
+        v_cpu, dt, ref = time_oracle(dims, cap, ofs, pins, sofs, sids, nthreads, keep=True)
         cpu = {"value": v_cpu, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"every {stride}th batch of the plan ({nsel} batches, {len(sids)} nets, {dt:.1f} s)"}
+               "sample": f"one batch in {stride} of the plan ({nsel} batches, {len(sids)} nets, {dt:.1f} s)"}
         parity = sample_parity(R, sofs, sids, ref)
 
     if dist:
