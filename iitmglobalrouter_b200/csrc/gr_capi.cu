@@ -290,11 +290,11 @@ BatchView make_view(void *dev, int64_t total_n, const BatchInfo &bi) {
 // k_mst_large shared memory: per pin a 64-bit key, five ints and a float
 size_t mst_smem(int max_pins) { return (size_t)max_pins * (sizeof(unsigned long long) + 6 * sizeof(int)); }
 // whether a net of n pins keeps its n x n cost matrix in shared memory
-bool mst_mat_in_smem(int n) { return mst_smem(n) + (size_t)n * n * sizeof(float) <= (size_t)kMstSmemMax; }
+bool mst_mat_in_smem(int n) { return mst_smem(n) + (size_t)n * mst_ld(n) * sizeof(float) <= (size_t)kMstSmemMax; }
 // k_mst_cluster shared memory per CTA: partial minima, the block arrays and
 // its ceil(n/cs) matrix rows
 size_t mst_cluster_smem(int n, int cs) {
-    return (size_t)n * sizeof(unsigned long long) + mst_smem(n) + (size_t)((n + cs - 1) / cs) * n * sizeof(float);
+    return (size_t)n * sizeof(unsigned long long) + mst_smem(n) + (size_t)((n + cs - 1) / cs) * mst_ld(n) * sizeof(float);
 }
 // cluster size for nets of up to n pins (0: no cluster -- one CTA suffices
 // or the matrix needs global memory)
@@ -392,13 +392,13 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         if (items <= 0) return GR_OK;
         const int maxn = v.nl > 0 ? v.max_pins : kMstWarpPins;
         const bool in_smem = mst_mat_in_smem(maxn);
-        size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
+        size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * mst_ld(maxn) * sizeof(float) : 0);
         sm = sm > kQueueWarpSmem ? sm : kQueueWarpSmem;
         int blocks = c->sm_count * (sm <= 100 * 1024 ? 2 : 1);
         uint32_t *gmat = nullptr;
         if (!in_smem) {
             blocks = c->sm_count;
-            if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
+            if (c->mat.bytes < (size_t)blocks * maxn * mst_ld(maxn) * sizeof(float)) return GR_ERR_STATE;
             gmat = (uint32_t *)c->mat.p;
         }
         blocks = items < blocks ? items : blocks;
@@ -406,7 +406,7 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
         vv.max_pins = maxn;
         int pi = prof_begin(c, s);
         k_mst_queue<<<blocks, kQueueThreads, sm, s>>>(c->g, vv, pcost, mst, dist, c->d_status, gmat,
-                                                      (int64_t)maxn * maxn, c->d_queue, mo);
+                                                      (int64_t)maxn * mst_ld(maxn), c->d_queue, mo);
         prof_end(c, s, pi, GR_K_MST_LARGE);
         GR_CK(cudaGetLastError());
         return GR_OK;
@@ -469,16 +469,16 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
                                          c->d_status, first, cnt, mo));
         } else {
             const bool in_smem = mst_mat_in_smem(maxn);
-            const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * maxn * sizeof(float) : 0);
+            const size_t sm = mst_smem(maxn) + (in_smem ? (size_t)maxn * mst_ld(maxn) * sizeof(float) : 0);
             int blocks = cnt < c->sm_count * 8 ? cnt : c->sm_count * 8;
             uint32_t *gmat = nullptr;
             if (!in_smem) {
                 blocks = cnt < c->sm_count ? cnt : c->sm_count;
-                if (c->mat.bytes < (size_t)blocks * maxn * maxn * sizeof(float)) return GR_ERR_STATE;
+                if (c->mat.bytes < (size_t)blocks * maxn * mst_ld(maxn) * sizeof(float)) return GR_ERR_STATE;
                 gmat = (uint32_t *)c->mat.p;
             }
             k_mst_large<<<blocks, c->tune[part ? GR_TUNE_MST_BIG_THREADS : GR_TUNE_MST_MID_THREADS], sm, sp>>>(
-                c->g, vv, pcost, mst, dist, c->d_status, gmat, (int64_t)maxn * maxn, first, cnt, mo);
+                c->g, vv, pcost, mst, dist, c->d_status, gmat, (int64_t)maxn * mst_ld(maxn), first, cnt, mo);
         }
         prof_end(c, sp, pi, GR_K_MST_LARGE);
     }
@@ -529,7 +529,7 @@ int check_mst_smem(gr_ctx *c, int max_pins) {
 int ensure_mst_scratch(gr_ctx *c, int max_pins, cudaStream_t s) {
     if (max_pins <= kMstWarpPins || mst_mat_in_smem(max_pins)) return GR_OK;
     if (!c->tune[GR_TUNE_MST_QUEUE] && (max_pins <= kMstMidPins || mst_cluster_size(max_pins))) return GR_OK;
-    return ensure(c->mat, (size_t)c->sm_count * max_pins * max_pins * sizeof(float), s);
+    return ensure(c->mat, (size_t)c->sm_count * max_pins * mst_ld(max_pins) * sizeof(float), s);
 }
 
 // scratch for one batch of the given sizes
@@ -1534,7 +1534,7 @@ constexpr size_t kSsOrder = kSsNpin + sizeof(int32_t) * kStaticMaxNets;     // i
 constexpr size_t kSsPairOfs = kSsOrder + sizeof(int32_t) * kStaticMaxNets;  // int64 [nets]
 constexpr size_t kSsNodeOfs = kSsPairOfs + sizeof(int64_t) * kStaticMaxNets;
 constexpr size_t kSsMat = kSsNodeOfs + sizeof(int64_t) * kStaticMaxNets;    // float matrices
-static_assert(kSsMat % 256 == 0 && kSsMat + sizeof(float) * kStaticMaxPins * kStaticMaxPins <= kStaticScratchBytes,
+static_assert(kSsMat % 256 == 0 && kSsMat + sizeof(float) * kStaticMaxPins * mst_ld(kStaticMaxPins) <= kStaticScratchBytes,
               "static Boruvka scratch holds its tables and at least one largest matrix");
 
 }  // namespace
@@ -1685,7 +1685,7 @@ extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, cons
     // (as many CTAs as it holds, at most one per SM)
     if (n_small > 0) {
         v.max_pins = max_small;
-        const size_t smem = mst_smem(max_small) + (size_t)max_small * max_small * sizeof(float);
+        const size_t smem = mst_smem(max_small) + (size_t)max_small * mst_ld(max_small) * sizeof(float);
         const int blocks = n_small < sd.sms * 8 ? n_small : sd.sms * 8;
         k_mst_large<<<blocks, max_small <= kMstMidPins ? 128 : 512, smem, s>>>(
             GridC{}, v, d_pair_cost, d_mst_edges, d_net_dist, st, nullptr, 0, 0, n_small, MarkOut{});
@@ -1693,12 +1693,12 @@ extern "C" int gr_brvsk_build_static(const int32_t *h_npin, int32_t n_nets, cons
     }
     if (n_small < n_nets) {
         v.max_pins = max_large;
-        const size_t mat = (size_t)max_large * max_large * sizeof(float);
+        const size_t mat = (size_t)max_large * mst_ld(max_large) * sizeof(float);
         const size_t fit = (kStaticScratchBytes - kSsMat) / mat;
         int blocks = (int)(fit < (size_t)sd.sms ? fit : (size_t)sd.sms);
         blocks = n_nets - n_small < blocks ? n_nets - n_small : blocks;
         k_mst_large<<<blocks, 512, mst_smem(max_large), s>>>(GridC{}, v, d_pair_cost, d_mst_edges, d_net_dist, st,
-                                                             (uint32_t *)(sd.base + kSsMat), (int64_t)max_large * max_large,
+                                                             (uint32_t *)(sd.base + kSsMat), (int64_t)max_large * mst_ld(max_large),
                                                              n_small, n_nets - n_small, MarkOut{});
         GR_CK(cudaGetLastError());
     }

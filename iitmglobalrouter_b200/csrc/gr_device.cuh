@@ -19,6 +19,9 @@ constexpr int kLutMin = -256;  // cost LUT covers remaining capacity [-256, 1024
 constexpr int kLutMax = 1024;
 constexpr int kTableMaxCells = 1 << 20;  // nx*ny above this: direct Fenwick gathers
 constexpr int kMstMaxRounds = 40;
+// Row stride of a Boruvka cost matrix: odd, so that one thread per row
+// reading column u of consecutive rows hits 32 different shared-memory banks.
+__host__ __device__ constexpr int mst_ld(int n) { return n | 1; }
 constexpr int kMstWarpPins = 32;   // nets up to this size: one warp each
 constexpr int kMaxLayers = 32;     // layer sets are 64-bit masks
 

@@ -713,15 +713,21 @@ __device__ __forceinline__ int64_t pair_id(int a, int b) {
     return a > b ? (int64_t)a * (a - 1) / 2 + b : (int64_t)b * (b - 1) / 2 + a;
 }
 
-// Per-pin state of a block-level Boruvka, in shared memory.
+// Per-pin state of a block-level Boruvka, in shared memory. A root's key,
+// the minimum (cost bits, pair id) of its crossing pairs, is kept as two
+// 32-bit halves (kb, ki) and found in two passes of 32-bit atomicMin: the
+// least cost bits first, then the least pair id among the rows that reach
+// them -- the same minimum as one 64-bit key, without 64-bit atomics
+// (which contend badly when every row of a round posts to one root).
 struct MstArrays {
-    unsigned long long *key;  // per root: min (cost, pair id) of its crossing pairs
+    uint32_t *kb, *ki;  // per root: cost bits and pair id of its minimum
     int *comp, *sel, *par, *mx, *flag;
-    float *wrec;              // costs of a round's recorded edges, in order
+    float *wrec;        // costs of a round's recorded edges, in order
     __device__ static MstArrays carve(void *base, int maxn) {
         MstArrays a;
-        a.key = (unsigned long long *)base;
-        a.comp = (int *)(a.key + maxn);
+        a.kb = (uint32_t *)base;
+        a.ki = a.kb + maxn;
+        a.comp = (int *)(a.ki + maxn);
         a.sel = a.comp + maxn;
         a.par = a.sel + maxn;
         a.mx = a.par + maxn;
@@ -730,12 +736,18 @@ struct MstArrays {
         return a;
     }
     __device__ float *end(int maxn) const { return wrec + maxn; }
+    __device__ unsigned long long key(int r) const { return ((unsigned long long)kb[r] << 32) | ki[r]; }
+    // a scan's per-row result (cost bits, pair id); sel and par are free
+    // until the round's tail writes them
+    __device__ uint32_t *row_bits() const { return (uint32_t *)sel; }
+    __device__ uint32_t *row_id() const { return (uint32_t *)par; }
 };
 
 // One pin's scan: min key over its crossing pairs, as a warp (row = the
-// pin's cost bits to every other pin), posted to its root. Within a row the
-// pair id grows with u, so the minimum (cost, pair id) is the minimum
-// (cost bits, u); the pair id is formed for the winner only.
+// pin's cost bits to every other pin); the row's result is stored and its
+// cost bits posted to its root (first pass). Within a row the pair id grows
+// with u, so the minimum (cost, pair id) is the minimum (cost bits, u); the
+// pair id is formed for the winner only.
 __device__ __forceinline__ void mst_scan_row(const MstArrays &a, const uint32_t *row, int v, int n, int lane) {
     const unsigned FULL = 0xffffffffu;
     const int cv = a.comp[v];
@@ -757,8 +769,67 @@ __device__ __forceinline__ void mst_scan_row(const MstArrays &a, const uint32_t 
     }
     const uint32_t hi = __reduce_min_sync(FULL, bb);
     const uint32_t wu = __reduce_min_sync(FULL, bb == hi ? (uint32_t)bu : 0xffffffffu);
-    if (lane == 0 && wu < (uint32_t)n)
-        atomicMin(a.key + cv, ((unsigned long long)hi << 32) | (unsigned long long)(uint32_t)pair_id(v, (int)wu));
+    if (lane == 0) {
+        a.row_bits()[v] = wu < (uint32_t)n ? hi : ~0u;
+        a.row_id()[v] = wu < (uint32_t)n ? (uint32_t)pair_id(v, (int)wu) : ~0u;
+        if (wu < (uint32_t)n) atomicMin(a.kb + cv, hi);
+    }
+}
+
+// The same scan for matrices in shared memory (rows r0..r1-1 of the net at
+// M + (v - r0) * ld, ld odd), by groups of T threads per row: T the largest
+// power of two up to 32 with (r1 - r0) * T <= B threads, thread j of a group
+// scanning columns j, j + T, ... and the group combining its (cost bits,
+// column) minima by shuffles, ties to the lower column -- the row's minimum
+// (cost bits, u) as in mst_scan_row, with fewer dependent steps per thread
+// when rows are few and short.
+__device__ __forceinline__ void mst_scan_rows_group(const MstArrays &a, const uint32_t *M, int ld, int r0, int r1,
+                                                    int n, int tid, int B) {
+    const unsigned FULL = 0xffffffffu;
+    const int rows = r1 - r0;
+    int T = 32;
+    while (T > 1 && rows * T > B) T >>= 1;
+    const int per = B / T, j = tid & (T - 1), gi = tid / T;
+    for (int base = r0; base < r1; base += per) {  // uniform over the block: every lane shuffles
+        const int v = base + gi;
+        uint32_t bb = ~0u;
+        int bu = n;
+        if (v < r1) {
+            const uint32_t *row = M + (int64_t)(v - r0) * ld;
+            const int cv = a.comp[v];
+            for (int u = j; u < n; u += T) {
+                const uint32_t c = row[u];
+                if (a.comp[u] != cv && c < bb) {
+                    bb = c;
+                    bu = u;
+                }
+            }
+        }
+        for (int o = T >> 1; o > 0; o >>= 1) {
+            const uint32_t ob = __shfl_xor_sync(FULL, bb, o);
+            const int ou = __shfl_xor_sync(FULL, bu, o);
+            if (ob < bb || (ob == bb && ou < bu)) {
+                bb = ob;
+                bu = ou;
+            }
+        }
+        if (v < r1 && j == 0) {
+            a.row_bits()[v] = bu < n ? bb : ~0u;
+            a.row_id()[v] = bu < n ? (uint32_t)pair_id(v, bu) : ~0u;
+            if (bu < n) atomicMin(a.kb + a.comp[v], bb);
+        }
+    }
+}
+
+// Second pass, after a barrier that follows every row's scan: the rows
+// v0, v0 + step, ... below v1 that reach their root's least cost bits post
+// their pair ids.
+__device__ __forceinline__ void mst_post_ids(const MstArrays &a, int v0, int v1, int step) {
+    for (int v = v0; v < v1; v += step) {
+        const uint32_t b = a.row_bits()[v];
+        const int cv = a.comp[v];
+        if (b != ~0u && b == a.kb[cv]) atomicMin(a.ki + cv, a.row_id()[v]);
+    }
 }
 
 // The rest of a round once a.key holds every root's minimum (gmst_util.hpp:
@@ -775,9 +846,9 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
     const int B = blockDim.x, tid = threadIdx.x;
     for (int v = tid; v < n; v += B) {
         int s = -1;
-        if (a.comp[v] == v && a.key[v] != ~0ull) {
+        if (a.comp[v] == v && a.kb[v] != ~0u) {
             int j, k;
-            pair_decode((long long)(uint32_t)a.key[v], j, k);
+            pair_decode((long long)a.ki[v], j, k);
             s = (a.comp[j] == v) ? a.comp[k] : a.comp[j];
         }
         a.sel[v] = s;
@@ -805,7 +876,7 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
     for (int v = c0; v < c1; v++)
         if (a.flag[v]) {
             if (out) out[nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)a.sel[v];
-            if (want_d) a.wrec[pos] = key_cost(a.key[v]);
+            if (want_d) a.wrec[pos] = key_cost(a.key(v));
             pos++;
         }
     __syncthreads();
@@ -841,9 +912,9 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
 __device__ __forceinline__ void mst_block_net(const GridC &g, const BatchView &bv, const MarkOut &mo,
                                               const float *__restrict__ cost, int64_t *__restrict__ mst,
                                               float *__restrict__ dist, uint32_t *status, const MstArrays &a,
-                                              uint32_t *M, int net, int *warp_sums, int *s_total) {
+                                              uint32_t *M, bool m_smem, int net, int *warp_sums, int *s_total) {
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
-    const int n = bv.npin[net];
+    const int n = bv.npin[net], ld = mst_ld(n);
     const long long P = (long long)n * (n - 1) / 2;
     const float *w = cost + bv.pair_ofs[net];
     int64_t *out = mst + bv.node_ofs[net];
@@ -860,8 +931,8 @@ __device__ __forceinline__ void mst_block_net(const GridC &g, const BatchView &b
             for (int i = 0; i < 4; i++) {
                 if (e + i * B < P) {
                     const uint32_t b = cost_bits(c[i]);
-                    M[j * n + k] = b;
-                    M[k * n + j] = b;
+                    M[j * ld + k] = b;
+                    M[k * ld + j] = b;
                 }
                 k += B;
                 while (k >= j) {
@@ -877,9 +948,13 @@ __device__ __forceinline__ void mst_block_net(const GridC &g, const BatchView &b
     __syncthreads();
     while (nrec < n - 1 && rounds < kMstMaxRounds) {
         rounds++;
-        for (int v = tid; v < n; v += B) a.key[v] = ~0ull;
+        for (int v = tid; v < n; v += B) a.kb[v] = a.ki[v] = ~0u;
         __syncthreads();
-        for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * n, v, n, lane);
+        if (m_smem) mst_scan_rows_group(a, M, ld, 0, n, n, tid, B);
+        else
+            for (int v = warp; v < n; v += nw) mst_scan_row(a, M + (int64_t)v * ld, v, n, lane);
+        __syncthreads();
+        mst_post_ids(a, tid, n, B);
         __syncthreads();
         nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, s_total, status, dist != nullptr);
     }
@@ -903,7 +978,8 @@ __global__ void __launch_bounds__(1024) k_mst_large(GridC g, BatchView bv, const
     const MstArrays a = MstArrays::carve(sm, maxn);
     uint32_t *M = gmat ? gmat + (int64_t)blockIdx.x * gmat_stride : (uint32_t *)a.end(maxn);
     for (int t = blockIdx.x; t < count; t += gridDim.x)
-        mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, bv.order[first + t], warp_sums, &s_total);
+        mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, gmat == nullptr, bv.order[first + t], warp_sums,
+                      &s_total);
 }
 
 // Nets whose n x n matrix exceeds one CTA's shared memory: a cluster of CS
@@ -920,14 +996,15 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int maxn = bv.max_pins;
-    unsigned long long *part = sm;  // this CTA's per-root minima over its rows
+    unsigned long long *part = sm;  // this CTA's per-root minima over its rows (bits, ids)
+    uint32_t *pb = (uint32_t *)part, *pi = pb + maxn;
     const MstArrays a = MstArrays::carve(part + maxn, maxn);
     uint32_t *M = (uint32_t *)a.end(maxn);
     const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
     const int ncl = gridDim.x / CS, cid = blockIdx.x / CS;
     for (int t = cid; t < count; t += ncl) {
         const int net = bv.order[first + t];
-        const int n = bv.npin[net];
+        const int n = bv.npin[net], ld = mst_ld(n);
         const int rn = (n + CS - 1) / CS, r0 = min(n, rank * rn), r1 = min(n, r0 + rn);
         const float *w = cost + bv.pair_ofs[net];
         // this CTA's rows as cost bits; four independent gathers in flight
@@ -941,8 +1018,10 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
                 c[i] = (idx < cnt && u != v) ? __ldg(w + pair_id(v, u)) : 0.0f;
             }
 #pragma unroll
-            for (int i = 0; i < 4; i++)
-                if (i0 + i * B < cnt) M[i0 + i * B] = cost_bits(c[i]);
+            for (int i = 0; i < 4; i++) {
+                const int idx = i0 + i * B, r = idx / n;
+                if (idx < cnt) M[r * ld + (idx - r * n)] = cost_bits(c[i]);
+            }
         }
         for (int v = tid; v < n; v += B) a.comp[v] = v;
         float d = 0.0f;
@@ -950,20 +1029,24 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
         __syncthreads();
         while (nrec < n - 1 && rounds < kMstMaxRounds) {
             rounds++;
-            for (int v = tid; v < n; v += B) part[v] = ~0ull;
+            for (int v = tid; v < n; v += B) pb[v] = pi[v] = ~0u;
             __syncthreads();
-            const MstArrays ap = {part, a.comp, a.sel, a.par, a.mx, a.flag, a.wrec};
-            for (int v = r0 + warp; v < r1; v += nw) mst_scan_row(ap, M + (int64_t)(v - r0) * n, v, n, lane);
+            const MstArrays ap = {pb, pi, a.comp, a.sel, a.par, a.mx, a.flag, a.wrec};
+            mst_scan_rows_group(ap, M, ld, r0, r1, n, tid, B);
+            __syncthreads();
+            mst_post_ids(ap, r0 + tid, r1, B);
             cl.sync();  // every CTA's partial minima final
             for (int v = tid; v < n; v += B) {
-                unsigned long long k = part[v];
+                unsigned long long k = ((unsigned long long)pb[v] << 32) | pi[v];
 #pragma unroll
                 for (int r = 0; r < CS; r++) {
                     if (r == rank) continue;
-                    const unsigned long long o = cl.map_shared_rank(part, r)[v];
+                    const unsigned long long o = ((unsigned long long)cl.map_shared_rank(pb, r)[v] << 32) |
+                                                 cl.map_shared_rank(pi, r)[v];
                     k = o < k ? o : k;
                 }
-                a.key[v] = k;
+                a.kb[v] = (uint32_t)(k >> 32);
+                a.ki[v] = (uint32_t)k;
             }
             cl.sync();  // remote reads done before the partials are reset
             nrec += mst_round_tail(a, n, net, nrec, rank == 0 ? mst + bv.node_ofs[net] : nullptr, d, warp_sums,
@@ -1338,29 +1421,40 @@ __device__ __forceinline__ void mst_warp_net(const GridC &g, const BatchView &bv
     }
     const float *w = sw;
     int64_t *out = mst + bv.node_ofs[i];
+    // each root's least (cost bits, pair id) in two 32-bit passes (as in
+    // MstArrays): cost bits in skb, then the least pair id among the lanes
+    // that reach them in ski
+    uint32_t *skb = (uint32_t *)skey, *ski = skb + 32;
     scomp[lane] = lane;
     int nrec = 0;
     float d = 0.0f;
     for (int round = 0; nrec < n - 1 && round < kMstMaxRounds; round++) {
-        skey[lane] = ~0ull;
+        skb[lane] = ~0u;
+        ski[lane] = ~0u;
         __syncwarp();
+        const int cv = scomp[lane];
+        uint32_t bb = ~0u, be = ~0u;
         if (lane < n) {
-            const int cv = scomp[lane];
-            unsigned long long best = ~0ull;
+            // pair ids grow with u along the row: the first least cost bits win
             for (int u = 0; u < n; u++) {
                 if (scomp[u] == cv) continue;
-                const int64_t e = pair_id(lane, u);
-                const unsigned long long kk = cost_key(w[e], (uint32_t)e);
-                best = kk < best ? kk : best;
+                const uint32_t e = (uint32_t)pair_id(lane, u);
+                const uint32_t c = cost_bits(w[e]);
+                if (c < bb) {
+                    bb = c;
+                    be = e;
+                }
             }
-            if (best != ~0ull) atomicMin(&skey[cv], best);
+            if (be != ~0u) atomicMin(&skb[cv], bb);
         }
         __syncwarp();
+        if (be != ~0u && bb == skb[cv]) atomicMin(&ski[cv], be);
+        __syncwarp();
         int sel = -1;
-        const unsigned long long mykey = skey[lane];
-        if (lane < n && scomp[lane] == lane && mykey != ~0ull) {
+        const unsigned long long mykey = ((unsigned long long)skb[lane] << 32) | ski[lane];
+        if (lane < n && scomp[lane] == lane && skb[lane] != ~0u) {
             int pj, pk;
-            pair_decode((long long)(uint32_t)mykey, pj, pk);
+            pair_decode((long long)ski[lane], pj, pk);
             sel = scomp[pj] == lane ? scomp[pk] : scomp[pj];
         }
         const int sel_of_sel = __shfl_sync(FULL, sel, sel < 0 ? 0 : sel);
@@ -1451,8 +1545,8 @@ __global__ void __launch_bounds__(kQueueThreads) k_mst_queue(GridC g, BatchView 
         if (item >= total) break;
         if (item < nlarge) {  // nets above 128 pins first, then 33..128
             const int t = item < nbig ? bv.nmid + item : item - nbig;
-            mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, bv.order[bv.n2 + bv.nm + t], warp_sums,
-                          &s_total);
+            mst_block_net(g, bv, mo, cost, mst, dist, status, a, M, gmat == nullptr, bv.order[bv.n2 + bv.nm + t],
+                          warp_sums, &s_total);
         } else {
             const int t = (item - nlarge) * kQueueWarps + warp;
             if (t < bv.nm)
