@@ -495,12 +495,15 @@ def main():
     kd = kernels[dominant]
     alg_per_launch = units[dominant][1] / kd["launches"]
     achieved = alg_per_launch / (kd["ms"] / kd["launches"] / 1e3) / 1e9
-    traffic = None
+    traffic = traffic_cold = None
     tf = ROOT / "profiles" / "dram_traffic.json"
     if tf.exists():
-        pu = json.loads(tf.read_text()).get("per_unit", {}).get(dominant)
-        if pu:
+        tj = json.loads(tf.read_text())
+        pu, pc = tj.get("per_unit", {}).get(dominant), tj.get("per_unit_cold", {}).get(dominant)
+        if pu:  # in situ: each kernel sees the L2 its predecessors left, as in the timed step
             traffic = pu["bytes"] * units[dominant][0] / kd["launches"]
+        if pc:  # every launch from a cold cache
+            traffic_cold = pc["bytes"] * units[dominant][0] / kd["launches"]
     # and of the whole step (all kernels, B_net summed over the nets)
     bnet = net_bytes(d, ofs, pins, int(demand.sum()))
     step_achieved = bnet / (ms_step / 1e3) / 1e9
@@ -554,7 +557,7 @@ def main():
                    "batches": len(bofs) - 1, "seed": args.seed, "parallelism": f"replicas x{world}",
                    "l2": "flushed (256 MB write) before every timed step", "graph": True, "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_source": peak_kind, "kernel": dominant,
+                     "traffic": traffic, "traffic_cold": traffic_cold, "peak_source": peak_kind, "kernel": dominant,
                      "algorithmic_bytes_per_launch": alg_per_launch,
                      "step": {"achieved": step_achieved, "frac": step_achieved / peak, "algorithmic_bytes": bnet}},
         "kernels": kernels,

@@ -129,7 +129,7 @@ def reduce(args) -> None:
             per_unit[k] = {"unit": KINDS[k], "bytes": round(a["bytes"] / u, 3), "launches": a["launches"],
                            "units": u, "dram_bytes": int(a["bytes"])}
     out = {"what": "DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic unit of each "
-                   "route kernel kind over the captured batches (ncu: caches flushed before every launch)",
+                   "route kernel kind over the captured batches",
            "workload": f"synthetic design config {meta['config']}, seed {meta['seed']}, batches "
                        f"{meta['batches'][0]}..{meta['batches'][1] - 1}",
            "per_unit": per_unit}
