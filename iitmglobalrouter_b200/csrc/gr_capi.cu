@@ -491,11 +491,13 @@ int launch_mst(gr_ctx *c, const BatchView &v, const float *pcost, int64_t *mst, 
     return GR_OK;
 }
 
-constexpr int kTrackWarps = 8;       // warps per k_track_commit block
+// warps per k_track_commit block: small blocks, so that a block held by one
+// heavily marked track keeps few finished warps' slots idle (2 warps: 50.0 ms
+// per route of the 1.2M-net design, against 50.1 with 4 and 50.2 with 8)
+constexpr int kTrackWarps = 2;
 static_assert(kTrackWarps <= kTrackWarpsMax, "k_track_commit's per-warp rank tables");
 // marked cells per track kept in shared memory (more go to the track's slice
-// of the global scratch): 16 KB per 8-warp block, so eight blocks fit an SM
-// and a batch's touched tracks (up to ~10K) run in one wave
+// of the global scratch): 4 KB per 2-warp block
 constexpr int kTrackCapMax = 256;
 
 size_t track_smem(int cap) { return (size_t)kTrackWarps * 2 * cap * sizeof(int32_t); }
@@ -510,7 +512,7 @@ int launch_commit(gr_ctx *c, const BatchView &v, const int64_t *mst, const int16
     }
     int pi = prof_begin(c, s);
     int64_t blocks = ((int64_t)c->n_tracks + kTrackWarps - 1) / kTrackWarps;
-    if (blocks > (int64_t)c->sm_count * 8) blocks = (int64_t)c->sm_count * 8;
+    if (blocks > (int64_t)c->sm_count * 32) blocks = (int64_t)c->sm_count * 32;
     k_track_commit<<<(int)blocks, kTrackWarps * 32, track_smem(c->track_cap), s>>>(
         c->g, c->n_tracks, c->d_mark, c->d_capr, c->d_dlut, c->d_fen, c->d_gpos, c->d_gdel, c->track_cap,
         c->la_on ? c->d_pred : nullptr, c->la_beta);
