@@ -670,9 +670,17 @@ __global__ void __launch_bounds__(256) k_lpat_pairs(GridC g, int csize, const in
 }
 
 // ---------------------------------------------------------------- Boruvka
-// Block-wide exclusive scan (blockDim.x multiple of 32, <= 1024).
-__device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Barrier of the first nt threads of the block (nt a multiple of 32): the
+// whole block's barrier when nt is the block size, else named barrier 1.
+__device__ __forceinline__ void sync_first(int nt) {
+    if (nt == (int)blockDim.x) __syncthreads();
+    else asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+}
+
+// Exclusive scan over the first nt threads of the block (nt a multiple of
+// 32, <= 1024); only those threads call it.
+__device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total, int nt) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = nt >> 5;
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -680,7 +688,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total
         if (lane >= o) x += y;
     }
     if (lane == 31) warp_sums[wid] = x;
-    __syncthreads();
+    sync_first(nt);
     if (wid == 0) {
         int s = lane < nw ? warp_sums[lane] : 0;
 #pragma unroll
@@ -690,11 +698,20 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_sums, int &total
         }
         warp_sums[lane] = s;
     }
-    __syncthreads();
+    sync_first(nt);
     int pre = wid > 0 ? warp_sums[wid - 1] : 0;
     total = warp_sums[nw - 1];
-    __syncthreads();
+    sync_first(nt);
     return pre + x - v;
+}
+
+// Threads that run a round's tail: one per pin rounded up to a warp, at
+// least 64 and at most 256 (or the block); the rest of the block skips the
+// tail's barriers and waits at one block barrier after it.
+__device__ __forceinline__ int tail_threads(int n) {
+    int t = ((n + 31) >> 5) << 5;
+    t = t < 64 ? 64 : (t > 256 ? 256 : t);
+    return t < (int)blockDim.x ? t : (int)blockDim.x;
 }
 
 // One CTA per net. Per round (gmst_util.hpp:518-533):
@@ -840,10 +857,11 @@ __device__ __forceinline__ void mst_post_ids(const MstArrays &a, int v0, int v1,
 // at the larger one), found by following each candidate's chain to its
 // tree's top. Returns the number of edges recorded this round. want_d false
 // (the caller keeps no per-net sums) skips the sum, a serial step of one
-// thread per round.
+// thread per round. Run by the first nt threads of the block only (their
+// own barriers); the caller synchronises the block afterwards.
 __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net, int nrec, int64_t *out, float &d,
-                                              int *warp_sums, int *s_total, uint32_t *status, bool want_d) {
-    const int B = blockDim.x, tid = threadIdx.x;
+                                              int *warp_sums, uint32_t *status, bool want_d, int nt) {
+    const int B = nt, tid = threadIdx.x;
     for (int v = tid; v < n; v += B) {
         int s = -1;
         if (a.comp[v] == v && a.kb[v] != ~0u) {
@@ -853,7 +871,7 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
         }
         a.sel[v] = s;
     }
-    __syncthreads();
+    sync_first(nt);
     for (int v = tid; v < n; v += B) {
         const int s = a.sel[v];
         if (s >= 0) {
@@ -866,20 +884,20 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
         }
         a.mx[v] = -1;
     }
-    __syncthreads();
+    sync_first(nt);
     const int chunk = (n + B - 1) / B;
     const int c0 = min(n, tid * chunk), c1 = min(n, c0 + chunk);
     int cnt = 0;
     for (int v = c0; v < c1; v++) cnt += a.flag[v];
     int total;
-    int pos = block_excl_scan(cnt, warp_sums, total);
+    int pos = block_excl_scan(cnt, warp_sums, total, nt);
     for (int v = c0; v < c1; v++)
         if (a.flag[v]) {
             if (out) out[nrec + pos] = ((int64_t)net << 30) | ((int64_t)v << 15) | (int64_t)a.sel[v];
             if (want_d) a.wrec[pos] = key_cost(a.key(v));
             pos++;
         }
-    __syncthreads();
+    sync_first(nt);
     if (want_d && tid == 0) {
         float dd = d;
         for (int i = 0; i < total; i++) dd += a.wrec[i];
@@ -896,12 +914,12 @@ __device__ __forceinline__ int mst_round_tail(const MstArrays &a, int n, int net
         a.flag[v] = p;  // flag[] is free again: it now holds the top
         atomicMax(a.mx + p, v);
     }
-    __syncthreads();
+    sync_first(nt);
     for (int u = tid; u < n; u += B) {
         const int r = a.comp[u];
         if (a.sel[r] >= 0) a.comp[u] = a.mx[a.flag[r]];
     }
-    __syncthreads();
+    sync_first(nt);
     return total;
 }
 
@@ -956,7 +974,14 @@ __device__ __forceinline__ void mst_block_net(const GridC &g, const BatchView &b
         __syncthreads();
         mst_post_ids(a, tid, n, B);
         __syncthreads();
-        nrec += mst_round_tail(a, n, net, nrec, out, d, warp_sums, s_total, status, dist != nullptr);
+        {
+            const int nt = tail_threads(n);
+            int t = 0;
+            if (tid < nt) t = mst_round_tail(a, n, net, nrec, out, d, warp_sums, status, dist != nullptr, nt);
+            if (tid == 0) *s_total = t;
+            __syncthreads();  // the merge visible to every warp
+            nrec += *s_total;
+        }
     }
     for (int v = nrec + tid; v < n; v += B) out[v] = -1;
     if (tid == 0) {
@@ -1049,8 +1074,16 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
                 a.ki[v] = (uint32_t)k;
             }
             cl.sync();  // remote reads done before the partials are reset
-            nrec += mst_round_tail(a, n, net, nrec, rank == 0 ? mst + bv.node_ofs[net] : nullptr, d, warp_sums,
-                                   &s_total, status, dist != nullptr);
+            {
+                const int nt = tail_threads(n);
+                int tt = 0;
+                if (tid < nt)
+                    tt = mst_round_tail(a, n, net, nrec, rank == 0 ? mst + bv.node_ofs[net] : nullptr, d, warp_sums,
+                                        status, dist != nullptr, nt);
+                if (tid == 0) s_total = tt;
+                __syncthreads();  // the merge visible to every warp
+                nrec += s_total;
+            }
         }
         if (rank == 0) {
             int64_t *out = mst + bv.node_ofs[net];
