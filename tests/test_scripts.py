@@ -112,3 +112,30 @@ def test_gather_bytes_matches_a_literal_walk():
                         pats += 1
     got = d.gather_bytes(threads=4)
     assert got["patterns"] == pats and got["bytes"] == 4 * total
+
+
+def test_traffic_reduce_per_unit(tmp_path):
+    """The profile helper's reduction: DRAM bytes of the captured launches of
+    each kernel kind over that kind's units (L-pattern variants are one kind,
+    the cluster Boruvka counts with k_mst_large)."""
+    from iitmglobalrouter_b200 import traffic
+
+    units = tmp_path / "u.json"
+    units.write_text(json.dumps({"config": 3, "seed": 1, "batches": [5, 6],
+                                 "units": {"k_lpat": 100, "k_mst_large": 50, "k_mst_warp": 0, "k_qtable": 10,
+                                           "k_track_commit": 20}}))
+    rows = ['"ID","Kernel Name","Metric Name","Metric Unit","Metric Value"']
+    for i, (k, rd, wr) in enumerate([("void k_lpat_z<10>(GridC)", 700, 0), ("void k_lpat_zs<10, 4>(GridC)", 300, 0),
+                                     ("k_mst_large(GridC)", 100, 0), ("void k_mst_cluster<4>(GridC)", 150, 50),
+                                     ("k_track_commit(GridC)", 400, 40), ("k_fen_tracks(GridC)", 9, 9)]):
+        rows.append(f'"{i}","{k}","dram__bytes_read.sum","byte","{rd}"')
+        rows.append(f'"{i}","{k}","dram__bytes_write.sum","byte","{wr}"')
+    csvf = tmp_path / "d.csv"
+    csvf.write_text("==PROF== noise\n" + "\n".join(rows) + "\n")
+    out = tmp_path / "o.json"
+    traffic.reduce(type("A", (), {"units": str(units), "csv": str(csvf), "out": str(out)})())
+    pu = json.loads(out.read_text())["per_unit"]
+    assert pu["k_lpat"]["bytes"] == 10.0 and pu["k_lpat"]["launches"] == 2
+    assert pu["k_mst_large"]["bytes"] == 6.0 and pu["k_mst_large"]["launches"] == 2
+    assert pu["k_track_commit"]["bytes"] == 22.0
+    assert "k_fen_tracks" not in pu and "k_mst_warp" not in pu
