@@ -10,6 +10,7 @@ by the L-pattern stage.
 from __future__ import annotations
 
 import ctypes as C
+from pathlib import Path
 
 import numpy as np
 
@@ -153,6 +154,49 @@ def snapshot_samples(design, fracs=(0.10, 0.25, 0.50, 0.75), num_xdim_parts=4, d
     return out
 
 
+def shard_seeds(n_designs: int, rank: int, world: int):
+    """The design seeds 1..n_designs that rank `rank` of `world` generates:
+    seed s goes to rank (s - 1) % world. The ranks share nothing, so the
+    training data of many designs is made one design per GPU with no
+    collective."""
+    return [s for s in range(1, n_designs + 1) if (s - 1) % world == rank]
+
+
+def write_shard(out_dir, n_designs: int, rank: int, world: int, make_samples) -> Path:
+    """Generates this rank's designs' samples with make_samples(seed) -> list
+    of (input, target) tensors and saves them, with their seeds, to
+    out_dir/shard_<rank>.npz."""
+    out = Path(out_dir)
+    out.mkdir(parents=True, exist_ok=True)
+    xs, ts, seeds = [], [], []
+    for s in shard_seeds(n_designs, rank, world):
+        for x, t in make_samples(s):
+            xs.append(x.detach().cpu().numpy())
+            ts.append(t.detach().cpu().numpy())
+            seeds.append(s)
+    path = out / f"shard_{rank}.npz"
+    if xs:
+        np.savez(path, x=np.stack(xs), t=np.stack(ts), seed=np.array(seeds, np.int32))
+    else:
+        np.savez(path, x=np.zeros((0,), np.float32), t=np.zeros((0,), np.float32), seed=np.zeros((0,), np.int32))
+    return path
+
+
+def load_shards(in_dir, device="cpu"):
+    """Every shard's samples, in design-seed order (within a design, in the
+    order they were made): the same list one process generating every seed
+    in turn would have made."""
+    import torch
+
+    parts = []
+    for f in sorted(Path(in_dir).glob("shard_*.npz")):
+        z = np.load(f)
+        for i in range(len(z["seed"])):
+            parts.append((int(z["seed"][i]), f.name, i, z["x"][i], z["t"][i]))
+    parts.sort(key=lambda r: (r[0], r[2]))
+    return [(torch.from_numpy(x).to(device), torch.from_numpy(t).to(device)) for _, _, _, x, t in parts]
+
+
 def train(net, samples, epochs=20, lr=1e-3, seed=0, log=None):
     """Adam on the samples, one sample per step, shuffled every epoch; returns the mean loss per epoch."""
     rng = np.random.default_rng(seed)
@@ -226,6 +270,12 @@ def main(argv=None):
     designs and compare plain and lookahead routing on held-out seeds.
 
         python -m iitmglobalrouter_b200.lookahead --designs 50 --epochs 20 --out weights.npy --report report.json
+
+    The samples can be made one design per GPU first (no collective; each
+    process writes its own shard), then trained on in one process:
+
+        torchrun --nproc-per-node 8 -m iitmglobalrouter_b200.lookahead --designs 50 --shard-dir shards
+        python -m iitmglobalrouter_b200.lookahead --samples-dir shards --epochs 20 --out weights.npy
     """
     import argparse
     import json
@@ -248,13 +298,31 @@ def main(argv=None):
     ap.add_argument("--report", default="")
     ap.add_argument("--weights", default="", help="evaluate these parameters instead of training")
     ap.add_argument("--mode", default="demand", choices=["demand", "excess"])
+    ap.add_argument("--shard-dir", default="",
+                    help="only make this rank's share of the training samples (RANK / WORLD_SIZE / LOCAL_RANK "
+                         "from the environment, one process per GPU) into this directory, then exit")
+    ap.add_argument("--samples-dir", default="", help="train on the shards in this directory")
     a = ap.parse_args(argv)
+    import os
+
+    if a.shard_dir:
+        import torch
+
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+        dev = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(dev)
+        path = write_shard(a.shard_dir, a.designs, rank, world,
+                           lambda s: snapshot_samples(Design.generate(a.config, seed=s, n_nets=a.nets), device=dev))
+        print(f"rank {rank}/{world}: {path}")
+        return {"shard": str(path)}
     t0 = time.time()
     d0 = Design.generate(a.config, seed=1, n_nets=a.nets).dims
     net = LookaheadNet(2 * d0["Z"], d0["Z"], d0["Y"], d0["X"], hidden=a.hidden, n_layers=a.layers, seed=7)
     samples, hist = [], []
     if a.weights:
         net.set_params(np.load(a.weights))
+    elif a.samples_dir:
+        samples = load_shards(a.samples_dir, device="cuda")
     else:
         for s in range(1, a.designs + 1):
             samples += snapshot_samples(Design.generate(a.config, seed=s, n_nets=a.nets))
