@@ -255,3 +255,24 @@ def test_lookahead_plan_graph_replays_and_restores_plain_cost(cuda):
         rc, mst_c, mp_c = g.route_batches(ofs, pins, bofs, ids, nthreads=8)
         assert rc == 0 and np.array_equal(mst.cpu().numpy(), mst_c) and np.array_equal(pat.cpu().numpy(), mp_c)
     assert R.status() == 0
+
+
+def test_sharded_samples_through_the_cli_train_like_one_process(cuda, tmp_path, monkeypatch):
+    """The training CLI's shard path on the GPU: two ranks' shards (made in
+    turn here, RANK / WORLD_SIZE set as torchrun would) hold exactly the
+    samples of one process making every seed, and training from them runs."""
+    import torch
+
+    for r in range(2):
+        monkeypatch.setenv("RANK", str(r))
+        monkeypatch.setenv("WORLD_SIZE", "2")
+        monkeypatch.setenv("LOCAL_RANK", "0")
+        lookahead.main(["--config", "1", "--designs", "3", "--nets", "400", "--shard-dir", str(tmp_path / "s")])
+    got = lookahead.load_shards(tmp_path / "s", device="cuda")
+    ref = [p for s in range(1, 4) for p in lookahead.snapshot_samples(gr.Design.generate(1, seed=s, n_nets=400))]
+    assert len(got) == len(ref) == 12
+    for (x, t), (xr, tr) in zip(got, ref):
+        assert torch.equal(x, xr) and torch.equal(t, tr)
+    rep = lookahead.main(["--config", "1", "--nets", "400", "--samples-dir", str(tmp_path / "s"), "--epochs", "2",
+                          "--hidden", "8", "--layers", "2", "--betas", "0,1", "--test-seeds", "9", "--every", "8"])
+    assert rep["samples"] == 12 and len(rep["loss"]) == 2
