@@ -30,9 +30,9 @@ NAMES = {
     GR_TUNE_MST_QUEUE: "mst_queue",
 }
 CANDIDATES = {
-    GR_TUNE_MST_MID_THREADS: [128, 256, 512, 1024],
+    GR_TUNE_MST_MID_THREADS: [128, 256, 384, 512, 768, 1024],
     GR_TUNE_MST_BIG_THREADS: [256, 512, 1024],
-    GR_TUNE_MST_CLUSTER_THREADS: [256, 512, 1024],
+    GR_TUNE_MST_CLUSTER_THREADS: [256, 384, 512, 768, 1024],
     GR_TUNE_MST_CLUSTER_MIN_PINS: [0, 129, 160, 192],
     GR_TUNE_LPAT_SPLIT: [0, 1, 2, 4],
     GR_TUNE_MST_QUEUE: [0, 1],
