@@ -1025,7 +1025,7 @@ __global__ void __launch_bounds__(1024) k_mst_cluster(GridC g, BatchView bv, con
     uint32_t *pb = (uint32_t *)part, *pi = pb + maxn;
     const MstArrays a = MstArrays::carve(part + maxn, maxn);
     uint32_t *M = (uint32_t *)a.end(maxn);
-    const int B = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = B >> 5;
+    const int B = blockDim.x, tid = threadIdx.x;
     const int ncl = gridDim.x / CS, cid = blockIdx.x / CS;
     for (int t = cid; t < count; t += ncl) {
         const int net = bv.order[first + t];
