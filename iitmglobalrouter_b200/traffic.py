@@ -82,6 +82,9 @@ def route(args) -> None:
     R = gr.Router(dims["X"], dims["Y"], dims["Z"], d.caps())
     R.set_nets(ofs, pins)
     R.plan_set(bofs, ids)
+    from . import tune
+
+    tune.apply(R, tune.load(tune.key(R)))  # the benchmark's launch shapes, when cached for this GPU and Z
     mst = torch.empty(R.plan_slots, dtype=torch.int64, device="cuda")
     pat = torch.empty(R.plan_slots, dtype=torch.int32, device="cuda")
     units = {k: 0 for k in KINDS}
