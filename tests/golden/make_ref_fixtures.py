@@ -181,8 +181,8 @@ def pack(src: Path, dst: Path = HERE, only=None, dirname=None):
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("step", choices=["run", "pack"])
-    ap.add_argument("--out", default="gpurun_out/ref")
-    ap.add_argument("--src", default="gpurun_out/ref")
+    ap.add_argument("--out", default="ref_runs")
+    ap.add_argument("--src", default="ref_runs")
     ap.add_argument("--only", nargs="*")
     a = ap.parse_args()
     if a.step == "run":
