@@ -513,3 +513,23 @@ def test_lpattern_split_bitexact(cuda, split):
         mst, mp = route_all_gpu(R, ofs, bofs, ids, "plan")
         assert np.array_equal(mst, mst_c) and np.array_equal(mp, mp_c)
         assert np.array_equal(bits(R.fenwick()), bits(g.fenwick()))
+
+
+def test_traffic_helper_units(cuda, tmp_path):
+    """The profile helper's route: the units of the captured batches (pairs
+    per class from the plan, committed GCELLs from the demand they add) on a
+    small design, with the router's own demand as the check."""
+    import json
+
+    from iitmglobalrouter_b200 import traffic
+
+    out = tmp_path / "u.json"
+    traffic.route(type("A", (), {"config": 1, "seed": 1, "batches": "2:4", "units": str(out)})())
+    u = json.loads(out.read_text())["units"]
+    d = gr.Design.generate(1, seed=1)
+    ofs, pins = d.nets()
+    bofs, ids = d.batch(4)
+    pairs = gr.pair_count(ofs, ids[bofs[2]:bofs[4]])
+    assert u["k_lpat"] == pairs > 0
+    assert u["k_mst_large"] + u["k_mst_warp"] <= pairs and u["k_qtable"] > 0
+    assert u["k_track_commit"] > 0
