@@ -110,29 +110,12 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
         }
 }
 
-// ------------------------------------------------------------------ forward convolution on tcgen05
-// One CTA computes a tile of 8 x 16 positions (128) x Nt (16 or 32) output
-// channels of a layer as an implicit GEMM. The tile's input with its one-cell
-// halo, 10 x 18 cells of every channel (rounded up to a multiple of 8
-// channels), is loaded once into shared memory as bf16 (zero outside the
-// grid); the 128 x Kp patch matrix is built from it in shared memory in the
-// canonical K-major layout without swizzle (8-row x 16-byte core matrices;
-// core matrix (row group g, k chunk c) at c * LBO + g * 128 bytes), the
-// weights likewise as an Nt x Kp matrix; one thread issues the Kp / 16
-// tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator of 128 lanes x Nt
-// columns in tensor memory) and commits them to an mbarrier; the epilogue
-// reads the accumulator with tcgen05.ld (warp w: lanes 32 (w % 4) .., columns
-// 16 (w / 4) ..), adds the bias, applies ReLU and writes Y[n][y][x] (rows of
-// 16 positions) and, when training, the pre-activation Z[m][n].
+// ------------------------------------------------------------------ tcgen05 helpers
+// (used by the forward / input-gradient convolution k_conv_strip and the
+// weight-gradient kernel k_wgrad_tc below)
 constexpr int kConvThreads = 256, kConvRows = 128, kConvTmemCols = 32;
-constexpr int kConvTY = 8, kConvTX = 16, kHaloY = kConvTY + 2, kHaloX = kConvTX + 2, kHalo = kHaloY * kHaloX;
 constexpr int kConvSmemMax = 200 * 1024;
 constexpr long long kConvWaitLimit = 1ll << 24;  // mbarrier polls before the kernel reports a stall
-
-__host__ __device__ constexpr int conv_halo_bytes(int cin) { return ((cin + 7) / 8) * 8 * kHalo * 2; }
-__host__ __device__ constexpr int conv_smem_bytes(int Kp, int Nt, int cin) {
-    return 1024 + kConvRows * Kp * 2 + Nt * Kp * 2 + conv_halo_bytes(cin) + 64;
-}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -178,20 +161,46 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
 
-__global__ void __launch_bounds__(kConvThreads, 2)
-    k_conv_tc(int cin, int cout, int H, int W, int Kp, int Nt, int Np, const float *__restrict__ X,
-              const __nv_bfloat16 *__restrict__ Wt, const float *__restrict__ bias, float *__restrict__ Y,
-              float *__restrict__ Zp, int relu, int *__restrict__ err) {
+// ------------------------------------------------------------------ forward convolution on tcgen05
+// A 3 x 3 convolution as an implicit GEMM with no patch matrix. A CTA computes a strip of 128
+// positions of one grid row (x0 .. x0 + 127 of row y) x Nt output channels.
+// Its input halo -- rows y - 1 .. y + 1, columns x0 - 1 .. x0 + 128, every
+// channel rounded up to a multiple of 16 -- is stored as bf16 in planes of 8
+// channels: plane c, halo row r, column q at ((c * 3 + r) * 130 + q) * 16
+// bytes, the 8 channels of a cell as one 16-byte row. In that layout the
+// 128 x 16 A operand of tap (dy, dx) and channel pair (2s, 2s + 1) is a
+// canonical no-swizzle K-major matrix as it lies: 8-row core matrices of
+// consecutive columns (stride 128 B), the second 8 channels one plane on
+// (LBO = 3 * 130 * 16 B), starting at plane 2s, row dy, column dx. So one
+// thread issues 9 taps x (channels / 16) MMAs straight from the halo into
+// one FP32 accumulator (128 lanes x Nt columns of tensor memory); the
+// weights of tap t are an Nt x channels matrix W[n][ci * 9 + t] in the same
+// layout. The epilogue reads the accumulator with tcgen05.ld (warp w: lanes
+// 32 (w % 4) .., columns 16 (w / 4) ..), adds the bias, applies ReLU and
+// writes Y[n][y][x] (32 consecutive positions per warp) and, when training,
+// the pre-activation Z[m][n].
+constexpr int kStripX = 128, kStripCols = kStripX + 2;
+
+__host__ __device__ constexpr int strip_cpad(int cin) { return (cin + 15) / 16 * 16; }
+__host__ __device__ constexpr int strip_smem_bytes(int Nt, int cin) {
+    return 1024 + strip_cpad(cin) / 8 * 3 * kStripCols * 16 + 9 * Nt * strip_cpad(cin) * 2 + 64;
+}
+
+__global__ void __launch_bounds__(kConvThreads)
+    k_conv_strip(int cin, int cout, int H, int W, int Kp, int Nt, int Np, const float *__restrict__ X,
+                 const __nv_bfloat16 *__restrict__ Wt, const float *__restrict__ bias, float *__restrict__ Y,
+                 float *__restrict__ Zp, int relu, int *__restrict__ err) {
     extern __shared__ uint8_t conv_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)conv_raw + 1023) & ~(uintptr_t)1023);
-    uint8_t *As = base;                                   // 128 x Kp
-    uint8_t *Bs = As + kConvRows * Kp * 2;                // Nt x Kp
-    __nv_bfloat16 *halo = (__nv_bfloat16 *)(Bs + Nt * Kp * 2);  // [channel][10][18]
-    uint64_t *bar = (uint64_t *)((uint8_t *)halo + conv_halo_bytes(cin));  // 8-byte aligned
+    const int cpad = strip_cpad(cin), nplanes = cpad / 8;
+    constexpr int kPlane = 3 * kStripCols * 16;  // bytes of one 8-channel plane
+    uint8_t *halo = base;                                     // nplanes x 3 x 130 x 16 B
+    uint8_t *Bs = halo + nplanes * kPlane;                    // 9 taps x (nplanes x Nt x 16 B)
+    uint64_t *bar = (uint64_t *)(Bs + 9 * Nt * cpad * 2);     // 8-byte aligned
     uint32_t *tmem_slot = (uint32_t *)(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int M = H * W, y0 = blockIdx.y * kConvTY, x0 = blockIdx.x * kConvTX;
-    const int nchunk = Kp >> 3;
+    const int M = H * W, y = blockIdx.y, x0 = blockIdx.x * kStripX;
+    const int tapB = nplanes * Nt * 16;  // bytes of one tap's weights
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tmem_slot)),
@@ -203,70 +212,39 @@ __global__ void __launch_bounds__(kConvThreads, 2)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-
-    // weights: B(n, k) = Wt[k][n] for n < Np, zero beyond
-    for (int i = tid; i < Nt * nchunk; i += kConvThreads) {
-        const int n = i % Nt, c = i / Nt;
+    // weights: tap t, plane c, row n: channels 8c .. 8c + 7 of W[n][ci * 9 + t]
+    for (int i = tid; i < 9 * nplanes * Nt; i += kConvThreads) {
+        const int t = i / (nplanes * Nt), rem = i - t * (nplanes * Nt), c = rem / Nt, n = rem - c * Nt;
         uint32_t w[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const int k = 8 * c + 2 * j;
+            const int ci0 = 8 * c + 2 * j, ci1 = ci0 + 1;
             const __nv_bfloat16 z = __float2bfloat16(0.0f);
-            const __nv_bfloat16 lo = n < Np ? Wt[(long long)k * Np + n] : z;
-            const __nv_bfloat16 hi = n < Np ? Wt[(long long)(k + 1) * Np + n] : z;
+            const __nv_bfloat16 lo = (n < Np && ci0 < cin) ? Wt[(long long)(ci0 * 9 + t) * Np + n] : z;
+            const __nv_bfloat16 hi = (n < Np && ci1 < cin) ? Wt[(long long)(ci1 * 9 + t) * Np + n] : z;
             w[j] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
         }
-        *(uint4 *)(Bs + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        *(uint4 *)(Bs + (size_t)t * tapB + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
-
-    // the halo tile: rows y0 - 1 .. y0 + 8, columns x0 - 1 .. x0 + 16, channels
-    // up to the next multiple of 8 (the extra ones zero)
-    const int ngroups = (cin + 7) >> 3;
-    const int nhalo = ngroups * 8 * kHalo;
-    for (int i0 = tid; i0 < nhalo; i0 += 8 * kConvThreads) {  // eight loads in flight per thread
+    // the halo: one cell (plane, row, column) of 8 channels per step, eight
+    // channel loads of a column in flight, coalesced along the columns
+    for (int i = tid; i < nplanes * 3 * kStripCols; i += kConvThreads) {
+        const int c = i / (3 * kStripCols), rem = i - c * 3 * kStripCols, r = rem / kStripCols, q = rem - r * kStripCols;
+        const int gy = y - 1 + r, gx = x0 - 1 + q;
+        const bool in = gy >= 0 && gy < H && gx >= 0 && gx < W;
         float v[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int i = i0 + u * kConvThreads;
-            const int ci = i / kHalo, rem = i - ci * kHalo, hy = rem / kHaloX, hx = rem - hy * kHaloX;
-            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
-            v[u] = (i < nhalo && ci < cin && gy >= 0 && gy < H && gx >= 0 && gx < W)
-                       ? __ldg(X + (long long)ci * M + gy * W + gx)
-                       : 0.0f;
+        for (int j = 0; j < 8; j++) {
+            const int ci = 8 * c + j;
+            v[j] = (in && ci < cin) ? __ldg(X + (long long)ci * M + gy * W + gx) : 0.0f;
         }
+        uint32_t w[4];
 #pragma unroll
-        for (int u = 0; u < 8; u++)
-            if (i0 + u * kConvThreads < nhalo) halo[i0 + u * kConvThreads] = __float2bfloat16(v[u]);
-    }
-    __syncthreads();
-    // patches: thread (row r = ty * 16 + tx, half h) fills the channel groups
-    // g = h, h + 2, ... of row r from the halo. A group of 8 channels is 72 k
-    // values = 9 whole chunks, so every element's halo offset and word
-    // position are compile-time constants; chunks past Kp are not stored.
-    {
-        const int r = tid & (kConvRows - 1), h = tid >> 7;
-        const int ty = r / kConvTX, tx = r - ty * kConvTX;
-        const uint16_t *hrow = reinterpret_cast<const uint16_t *>(halo) + ty * kHaloX + tx;
-        uint8_t *arow = As + r * 16;
-        for (int gi = h; gi < ngroups; gi += 2) {
-            const uint16_t *hg = hrow + gi * 8 * kHalo;
-            uint32_t w[4];
-#pragma unroll
-            for (int e = 0; e < 72; e += 2) {
-                const int j0 = e / 9, t0 = e % 9, j1 = (e + 1) / 9, t1 = (e + 1) % 9;
-                const uint32_t lo = hg[j0 * kHalo + (t0 / 3) * kHaloX + t0 % 3];
-                const uint32_t hi = hg[j1 * kHalo + (t1 / 3) * kHaloX + t1 % 3];
-                w[(e >> 1) & 3] = lo | (hi << 16);
-                if (((e >> 1) & 3) == 3) {
-                    const int c = gi * 9 + (e >> 3);
-                    if (c < nchunk)
-                        *(uint4 *)(arow + (size_t)c * (kConvRows * 16)) = make_uint4(w[0], w[1], w[2], w[3]);
-                }
-            }
+        for (int j = 0; j < 4; j++) {
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            w[j] = *reinterpret_cast<const uint32_t *>(&h2);
         }
-        // zero chunks past the last group (Kp = 80 for cin = 8, say)
-        for (int c = (ngroups * 9) + h; c < nchunk; c += 2)
-            *(uint4 *)(arow + (size_t)c * (kConvRows * 16)) = make_uint4(0u, 0u, 0u, 0u);
+        *(uint4 *)(halo + (size_t)i * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -276,18 +254,22 @@ __global__ void __launch_bounds__(kConvThreads, 2)
 
     if (tid == 0) {
         const uint32_t idesc = umma_idesc_bf16(kConvRows, Nt);
-        const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
-        const uint32_t a_lbo = kConvRows * 16, b_lbo = Nt * 16;
-        for (int s = 0; s < (Kp >> 4); s++) {
-            const uint64_t ad = umma_sdesc(a0 + 2 * s * a_lbo, a_lbo, 128);
-            const uint64_t bd = umma_sdesc(b0 + 2 * s * b_lbo, b_lbo, 128);
-            const uint32_t acc = s > 0;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-                : "memory");
+        const uint32_t h0 = smem_u32(halo), b0 = smem_u32(Bs);
+        int issued = 0;
+        for (int t = 0; t < 9; t++) {
+            const int dy = t / 3, dx = t % 3;
+            for (int s = 0; s < cpad / 16; s++) {
+                const uint64_t ad = umma_sdesc(h0 + (uint32_t)(2 * s * kPlane + (dy * kStripCols + dx) * 16), kPlane, 128);
+                const uint64_t bd = umma_sdesc(b0 + (uint32_t)(t * tapB + 2 * s * Nt * 16), Nt * 16, 128);
+                const uint32_t acc = issued > 0;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+                issued++;
+            }
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                          smem_u32(bar))
@@ -301,9 +283,8 @@ __global__ void __launch_bounds__(kConvThreads, 2)
     if (done && 16 * half < Nt) {
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * half, v);
-        const int r = 32 * q + lane, yy = y0 + r / kConvTX, xx = x0 + r % kConvTX;
-        const int m = yy * W + xx;
-        if (yy < H && xx < W) {
+        const int xx = x0 + 32 * q + lane, m = y * W + xx;
+        if (xx < W) {
 #pragma unroll
             for (int j = 0; j < 16; j++) {
                 const int n = 16 * half + j;
@@ -636,12 +617,13 @@ int pack_all(gr_cnn *c) {
 }
 
 // tiles of 16 columns x 8 rows
-dim3 conv_grid(const gr_cnn *c) { return dim3((c->W + kConvTX - 1) / kConvTX, (c->H + kConvTY - 1) / kConvTY); }
 
 // the tensor-core convolution takes a layer whose tiles fit in shared memory
 bool conv_tc_fits(const gr_cnn *c, int l) {
-    return conv_smem_bytes(c->Kp[l], round_up(c->cout[l], 16), c->cin[l]) <= kConvSmemMax;
+    return strip_smem_bytes(round_up(c->cout[l], 16), c->cin[l]) <= kConvSmemMax && round_up(c->cout[l], 16) <= 32;
 }
+
+dim3 strip_grid(const gr_cnn *c) { return dim3((c->W + kStripX - 1) / kStripX, c->H); }
 
 int forward(gr_cnn *c, cudaStream_t s) {
     const int M = c->H * c->W;
@@ -649,7 +631,7 @@ int forward(gr_cnn *c, cudaStream_t s) {
         const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
         if (conv_tc_fits(c, l)) {
             const int Nt = round_up(c->cout[l], 16);
-            k_conv_tc<<<conv_grid(c), kConvThreads, conv_smem_bytes(c->Kp[l], Nt, c->cin[l]), s>>>(
+            k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(Nt, c->cin[l]), s>>>(
                 c->cin[l], c->cout[l], c->H, c->W, c->Kp[l], Nt, c->Np[l], c->act[l], c->wt[l], bl, c->act[l + 1],
                 nullptr, l + 1 < c->n_layers, c->err);
             continue;
@@ -683,7 +665,7 @@ int backward(gr_cnn *c, const float *d_target) {
         k_wgrad_tc<<<dim3(splits, ktiles), kConvThreads, wgrad_smem_bytes(Nt), s>>>(cin, co, c->H, c->W, Nt, per,
                                                                                    c->act[l], dY, g, c->err);
         if (l > 0) {  // cin = hidden <= 32 and cout <= 32: always within the tensor-core tile
-            k_conv_tc<<<conv_grid(c), kConvThreads, conv_smem_bytes(c->KpT[l], round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
+            k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
                              dX, nullptr, 0, c->err);
             float *t = dY;
             dY = dX;
@@ -720,7 +702,7 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
     *out = nullptr;
     CN_CK(cudaSetDevice(device));
     // the attribute holds for the whole process: one constant value
-    CN_CK(cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
+    CN_CK(cudaFuncSetAttribute(k_conv_strip, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmemMax));
     gr_cnn *c = new gr_cnn();
     c->device = device;
     c->H = H;
