@@ -186,9 +186,29 @@ __host__ __device__ constexpr int strip_smem_bytes(int Nt, int cin) {
     return 1024 + strip_cpad(cin) / 8 * 3 * kStripCols * 16 + 9 * Nt * strip_cpad(cin) * 2 + 64;
 }
 
+// The shared-memory image of k_conv_strip's weights from Wt[k][n] (k = ci * 9
+// + t): tap t, plane c, row n holds channels 8c .. 8c + 7 of W[n][ci * 9 + t]
+// (zero past cin and past Np), 16 bytes per (t, c, n).
+__global__ void k_pack_strip(int cin, int Nt, int Np, const __nv_bfloat16 *__restrict__ Wt, uint4 *__restrict__ out) {
+    const int nplanes = strip_cpad(cin) / 8;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 9 * nplanes * Nt; i += gridDim.x * blockDim.x) {
+        const int t = i / (nplanes * Nt), rem = i - t * (nplanes * Nt), c = rem / Nt, n = rem - c * Nt;
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int ci0 = 8 * c + 2 * j, ci1 = ci0 + 1;
+            const __nv_bfloat16 z = __float2bfloat16(0.0f);
+            const __nv_bfloat16 lo = (n < Np && ci0 < cin) ? Wt[(long long)(ci0 * 9 + t) * Np + n] : z;
+            const __nv_bfloat16 hi = (n < Np && ci1 < cin) ? Wt[(long long)(ci1 * 9 + t) * Np + n] : z;
+            w[j] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+        }
+        out[i] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
 __global__ void __launch_bounds__(kConvThreads)
-    k_conv_strip(int cin, int cout, int H, int W, int Kp, int Nt, int Np, const float *__restrict__ X,
-                 const __nv_bfloat16 *__restrict__ Wt, const float *__restrict__ bias, float *__restrict__ Y,
+    k_conv_strip(int cin, int cout, int H, int W, int Nt, int Np, const float *__restrict__ X,
+                 const uint4 *__restrict__ Wimg, const float *__restrict__ bias, float *__restrict__ Y,
                  float *__restrict__ Zp, int relu, int *__restrict__ err) {
     extern __shared__ uint8_t conv_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)conv_raw + 1023) & ~(uintptr_t)1023);
@@ -212,20 +232,8 @@ __global__ void __launch_bounds__(kConvThreads)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    // weights: tap t, plane c, row n: channels 8c .. 8c + 7 of W[n][ci * 9 + t]
-    for (int i = tid; i < 9 * nplanes * Nt; i += kConvThreads) {
-        const int t = i / (nplanes * Nt), rem = i - t * (nplanes * Nt), c = rem / Nt, n = rem - c * Nt;
-        uint32_t w[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int ci0 = 8 * c + 2 * j, ci1 = ci0 + 1;
-            const __nv_bfloat16 z = __float2bfloat16(0.0f);
-            const __nv_bfloat16 lo = (n < Np && ci0 < cin) ? Wt[(long long)(ci0 * 9 + t) * Np + n] : z;
-            const __nv_bfloat16 hi = (n < Np && ci1 < cin) ? Wt[(long long)(ci1 * 9 + t) * Np + n] : z;
-            w[j] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-        }
-        *(uint4 *)(Bs + (size_t)t * tapB + (size_t)c * Nt * 16 + n * 16) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
+    // the weights' shared-memory image, packed once per parameter update (k_pack_strip)
+    for (int i = tid; i < 9 * nplanes * Nt; i += kConvThreads) reinterpret_cast<uint4 *>(Bs)[i] = __ldg(Wimg + i);
     // the halo: one cell (plane, row, column) of 8 channels per step, eight
     // channel loads of a column in flight, coalesced along the columns
     for (int i = tid; i < nplanes * 3 * kStripCols; i += kConvThreads) {
@@ -581,6 +589,8 @@ struct gr_cnn {
     float *params = nullptr, *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
     __nv_bfloat16 *wt[kMaxLayers] = {};
     __nv_bfloat16 *wf[kMaxLayers] = {};  // backward operand: Wf[co*9 + t][ci] = W[co][ci][8 - t]
+    uint4 *ws[kMaxLayers] = {};   // k_conv_strip's weight image of wt (forward)
+    uint4 *wfs[kMaxLayers] = {};  // and of wf (input gradient)
     int KpT[kMaxLayers] = {}, NpT[kMaxLayers] = {};
     float *zero_bias = nullptr;
     float *act[kMaxLayers + 1] = {};  // act[0] = input, act[l+1] = output of layer l
@@ -608,9 +618,15 @@ int pack_all(gr_cnn *c) {
     for (int l = 0; l < c->n_layers; l++) {
         k_pack_w<<<grid((long long)c->Kp[l] * c->Np[l]), 256, 0, c->stream>>>(c->cin[l], c->cout[l], c->Kp[l], c->Np[l],
                                                                                c->params + c->w_ofs[l], c->wt[l]);
-        if (l > 0)
+        if (c->ws[l])
+            k_pack_strip<<<grid(9LL * strip_cpad(c->cin[l]) / 8 * round_up(c->cout[l], 16)), 256, 0, c->stream>>>(
+                c->cin[l], round_up(c->cout[l], 16), c->Np[l], c->wt[l], c->ws[l]);
+        if (l > 0) {
             k_pack_wflip<<<grid((long long)c->KpT[l] * c->NpT[l]), 256, 0, c->stream>>>(
                 c->cin[l], c->cout[l], c->KpT[l], c->NpT[l], c->params + c->w_ofs[l], c->wf[l]);
+            k_pack_strip<<<grid(9LL * strip_cpad(c->cout[l]) / 8 * round_up(c->cin[l], 16)), 256, 0, c->stream>>>(
+                c->cout[l], round_up(c->cin[l], 16), c->NpT[l], c->wf[l], c->wfs[l]);
+        }
     }
     CN_CK(cudaGetLastError());
     return GR_OK;
@@ -632,8 +648,8 @@ int forward(gr_cnn *c, cudaStream_t s) {
         if (conv_tc_fits(c, l)) {
             const int Nt = round_up(c->cout[l], 16);
             k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(Nt, c->cin[l]), s>>>(
-                c->cin[l], c->cout[l], c->H, c->W, c->Kp[l], Nt, c->Np[l], c->act[l], c->wt[l], bl, c->act[l + 1],
-                nullptr, l + 1 < c->n_layers, c->err);
+                c->cin[l], c->cout[l], c->H, c->W, Nt, c->Np[l], c->act[l], c->ws[l], bl, c->act[l + 1], nullptr,
+                l + 1 < c->n_layers, c->err);
             continue;
         }
         k_im2col<<<grid((long long)M * c->Kp[l]), 256, 0, s>>>(c->cin[l], c->H, c->W, c->Kp[l], c->act[l], c->col);
@@ -665,7 +681,7 @@ int backward(gr_cnn *c, const float *d_target) {
         k_wgrad_tc<<<dim3(splits, ktiles), kConvThreads, wgrad_smem_bytes(Nt), s>>>(cin, co, c->H, c->W, Nt, per,
                                                                                    c->act[l], dY, g, c->err);
         if (l > 0) {  // cin = hidden <= 32 and cout <= 32: always within the tensor-core tile
-            k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, c->KpT[l], round_up(cin, 16), c->NpT[l], dY, c->wf[l], c->zero_bias,
+            k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, round_up(cin, 16), c->NpT[l], dY, c->wfs[l], c->zero_bias,
                              dX, nullptr, 0, c->err);
             float *t = dY;
             dY = dX;
@@ -749,7 +765,11 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
         ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
     for (int l = 0; l < n_layers && ok; l++) {
         ok = cudaMalloc(&c->wt[l], sizeof(__nv_bfloat16) * c->Kp[l] * c->Np[l]) == cudaSuccess &&
-             cudaMalloc(&c->wf[l], sizeof(__nv_bfloat16) * c->KpT[l] * c->NpT[l]) == cudaSuccess;
+             cudaMalloc(&c->wf[l], sizeof(__nv_bfloat16) * c->KpT[l] * c->NpT[l]) == cudaSuccess &&
+             cudaMalloc(&c->ws[l], sizeof(uint4) * 9 * strip_cpad(c->cin[l]) / 8 * round_up(c->cout[l], 16)) ==
+                 cudaSuccess &&
+             cudaMalloc(&c->wfs[l], sizeof(uint4) * 9 * strip_cpad(c->cout[l]) / 8 * round_up(c->cin[l], 16)) ==
+                 cudaSuccess;
         if (ok && !conv_tc_fits(c, l)) ok = cudaMalloc(&c->z[l], sizeof(float) * M * c->Np[l]) == cudaSuccess;
     }
     if (!ok) {
@@ -788,6 +808,8 @@ int gr_cnn_destroy(gr_cnn *c) {
     for (int l = 0; l < kMaxLayers; l++) {
         cudaFree(c->wt[l]);
         cudaFree(c->wf[l]);
+        cudaFree(c->ws[l]);
+        cudaFree(c->wfs[l]);
         cudaFree(c->z[l]);
     }
     for (int l = 0; l <= kMaxLayers; l++) cudaFree(c->act[l]);
