@@ -68,9 +68,10 @@ def _bf16_round(a):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("H,W,cin,hidden,cout", [
-    (37, 29, 20, 32, 20),  # 9 tiles of 128 positions, the last ragged; Kp 192; 32 output columns
-    (16, 8, 32, 16, 10),  # exactly one tile; Kp 288; 16 output columns
-    (50, 50, 32, 32, 32),  # 20 tiles
+    (37, 29, 20, 32, 20),  # one ragged strip of 29 of 128 positions per row; 20 channels padded to 32; 32 output columns
+    (16, 8, 32, 16, 10),  # strips of 8 positions; 32 channels; 16 output columns
+    (50, 50, 32, 32, 32),  # 50 strips
+    (6, 300, 20, 16, 16),  # three strips per row, the last ragged (300 = 2 x 128 + 44)
 ])
 def test_forward_exact_on_binary_grid(cuda, H, W, cin, hidden, cout):
     """Inputs on multiples of 1/16 in [0, 4) and weights on multiples of 1/64
