@@ -209,7 +209,8 @@ __global__ void k_pack_strip(int cin, int Nt, int Np, const __nv_bfloat16 *__res
 __global__ void __launch_bounds__(kConvThreads)
     k_conv_strip(int cin, int cout, int H, int W, int Nt, int Np, const float *__restrict__ X,
                  const uint4 *__restrict__ Wimg, const float *__restrict__ bias, float *__restrict__ Y,
-                 float *__restrict__ Zp, int relu, int *__restrict__ err) {
+                 float *__restrict__ Zp, int relu, int *__restrict__ err, const uint4 *__restrict__ Xh,
+                 uint4 *__restrict__ Yh) {
     extern __shared__ uint8_t conv_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)conv_raw + 1023) & ~(uintptr_t)1023);
     const int cpad = strip_cpad(cin), nplanes = cpad / 8;
@@ -240,6 +241,11 @@ __global__ void __launch_bounds__(kConvThreads)
         const int c = i / (3 * kStripCols), rem = i - c * 3 * kStripCols, r = rem / kStripCols, q = rem - r * kStripCols;
         const int gy = y - 1 + r, gx = x0 - 1 + q;
         const bool in = gy >= 0 && gy < H && gx >= 0 && gx < W;
+        if (Xh) {  // the previous layer's channel-last bf16 copy: the cell is one 16-byte load
+            reinterpret_cast<uint4 *>(halo)[i] = in ? __ldg(Xh + (long long)(gy * W + gx) * nplanes + c)
+                                                    : make_uint4(0u, 0u, 0u, 0u);
+            continue;
+        }
         float v[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
@@ -296,11 +302,25 @@ __global__ void __launch_bounds__(kConvThreads)
 #pragma unroll
             for (int j = 0; j < 16; j++) {
                 const int n = 16 * half + j;
+                const float raw = v[j];
+                v[j] = 0.0f;  // becomes the layer's output (0 past cout)
                 if (n < cout) {
-                    const float o = v[j] + bias[n];
-                    Y[(long long)n * M + m] = relu ? fmaxf(o, 0.0f) : o;
-                    if (Zp) Zp[(long long)m * Np + n] = v[j];
+                    const float o = raw + bias[n];
+                    v[j] = relu ? fmaxf(o, 0.0f) : o;
+                    Y[(long long)n * M + m] = v[j];
+                    if (Zp) Zp[(long long)m * Np + n] = raw;
                 }
+            }
+            if (Yh) {  // and its channel-last bf16 copy for the next layer's halo: 16 channels, 32 bytes
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    w[j] = *reinterpret_cast<const uint32_t *>(&h2);
+                }
+                uint4 *dst = Yh + (long long)m * (Nt / 8) + 2 * half;
+                dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
             }
         }
     }
@@ -594,6 +614,7 @@ struct gr_cnn {
     int KpT[kMaxLayers] = {}, NpT[kMaxLayers] = {};
     float *zero_bias = nullptr;
     float *act[kMaxLayers + 1] = {};  // act[0] = input, act[l+1] = output of layer l
+    uint4 *act_h[kMaxLayers + 1] = {};  // act[l] (l >= 1) as channel-last bf16, rounded up to 16 channels
     float *z[kMaxLayers] = {};  // GEMM output of the fallback path
     __nv_bfloat16 *col = nullptr;  // patches of a layer too wide for the tensor-core tile (fallback)
     float *dact = nullptr, *dact2 = nullptr, *loss = nullptr;
@@ -647,9 +668,13 @@ int forward(gr_cnn *c, cudaStream_t s) {
         const float *bl = c->params + c->w_ofs[l] + (int64_t)c->cout[l] * c->cin[l] * 9;
         if (conv_tc_fits(c, l)) {
             const int Nt = round_up(c->cout[l], 16);
+            // the input's channel-last copy when the previous layer (a strip
+            // convolution) wrote one; this layer's copy for the next
+            const uint4 *xh = (l > 0 && conv_tc_fits(c, l - 1)) ? c->act_h[l] : nullptr;
+            uint4 *yh = l + 1 < c->n_layers ? c->act_h[l + 1] : nullptr;
             k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(Nt, c->cin[l]), s>>>(
                 c->cin[l], c->cout[l], c->H, c->W, Nt, c->Np[l], c->act[l], c->ws[l], bl, c->act[l + 1], nullptr,
-                l + 1 < c->n_layers, c->err);
+                l + 1 < c->n_layers, c->err, xh, yh);
             continue;
         }
         k_im2col<<<grid((long long)M * c->Kp[l]), 256, 0, s>>>(c->cin[l], c->H, c->W, c->Kp[l], c->act[l], c->col);
@@ -682,7 +707,7 @@ int backward(gr_cnn *c, const float *d_target) {
                                                                                    c->act[l], dY, g, c->err);
         if (l > 0) {  // cin = hidden <= 32 and cout <= 32: always within the tensor-core tile
             k_conv_strip<<<strip_grid(c), kConvThreads, strip_smem_bytes(round_up(cin, 16), co), s>>>(co, cin, c->H, c->W, round_up(cin, 16), c->NpT[l], dY, c->wfs[l], c->zero_bias,
-                             dX, nullptr, 0, c->err);
+                             dX, nullptr, 0, c->err, nullptr, nullptr);
             float *t = dY;
             dY = dX;
             dX = t;
@@ -763,6 +788,8 @@ int gr_cnn_create(gr_cnn **out, int device, int in_channels, int out_channels, i
          cudaMemsetAsync(c->err, 0, sizeof(int), c->stream) == cudaSuccess;
     for (int l = 0; l <= n_layers && ok; l++)
         ok = cudaMalloc(&c->act[l], sizeof(float) * M * (l == 0 ? in_channels : c->cout[l - 1])) == cudaSuccess;
+    for (int l = 1; l < n_layers && ok; l++)
+        ok = cudaMalloc(&c->act_h[l], sizeof(uint16_t) * M * round_up(c->cout[l - 1], 16)) == cudaSuccess;
     for (int l = 0; l < n_layers && ok; l++) {
         ok = cudaMalloc(&c->wt[l], sizeof(__nv_bfloat16) * c->Kp[l] * c->Np[l]) == cudaSuccess &&
              cudaMalloc(&c->wf[l], sizeof(__nv_bfloat16) * c->KpT[l] * c->NpT[l]) == cudaSuccess &&
@@ -812,7 +839,10 @@ int gr_cnn_destroy(gr_cnn *c) {
         cudaFree(c->wfs[l]);
         cudaFree(c->z[l]);
     }
-    for (int l = 0; l <= kMaxLayers; l++) cudaFree(c->act[l]);
+    for (int l = 0; l <= kMaxLayers; l++) {
+        cudaFree(c->act[l]);
+        cudaFree(c->act_h[l]);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return GR_OK;
